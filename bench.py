@@ -1,0 +1,434 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 batched 3D complex FFT.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints ONE JSON line.  The headline workload is 2048 volumes of 17x17x17
+complex128, uniform[-1,1) re/im, seeded: one step is a forward transform and the
+inverse (1/V) of the whole batch, device-resident (`value`, volumes/s), and the
+same step through the host-pointer C ABI with page-locked buffers, copies
+included (`e2e`).  `roofline` describes the forward 17^3 kernel: algorithmic
+bytes (read + write once, 2*16*4913 B per volume) over its CUDA-event time,
+against the measured HBM copy bandwidth.  `workloads` adds the same per-L
+measurement (volumes/s, fraction of HBM roofline) for the other plain
+configurations.  `cpu_baseline` is the reference's best single-core C kernels
+(bench/geom/best, built into oracle/_ref) on a bounded sample, all host threads.
+
+For N > 1 (torchrun, one rank per GPU) every rank transforms its own 2048
+volumes (weak scaling, no collective on the data path); time is the max over
+ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "opt-fft_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+L2_BYTES = 126 * 1024 * 1024
+
+WORKLOADS = {
+    "roundtrip17": dict(shape=(17, 17, 17), batch=2048, prec=0, chain=(-1, +1), dist="uniform",
+                        label="2048 x 17^3 complex128, forward then inverse (1/N)"),
+    "fwd8": dict(shape=(8, 8, 8), batch=4096, prec=0, chain=(-1,), dist="uniform",
+                 label="4096 x 8^3 complex128 forward"),
+    "fwd17": dict(shape=(17, 17, 17), batch=2048, prec=0, chain=(-1,), dist="uniform",
+                  label="2048 x 17^3 complex128 forward"),
+    "fwd36": dict(shape=(36, 36, 36), batch=256, prec=0, chain=(-1,), dist="normal",
+                  label="256 x 36^3 complex128 forward"),
+    "fwd16x16x32": dict(shape=(16, 16, 32), batch=1024, prec=0, chain=(-1,), dist="normal",
+                        label="1024 x 16x16x32 complex128 forward"),
+    "fwd8_c64": dict(shape=(8, 8, 8), batch=4096, prec=1, chain=(-1,), dist="uniform",
+                     label="4096 x 8^3 complex64 forward"),
+    "fwd16_c64": dict(shape=(16, 16, 16), batch=1024, prec=1, chain=(-1,), dist="uniform",
+                      label="1024 x 16^3 complex64 forward"),
+}
+EXTRA = ["fwd8", "fwd17", "fwd36", "fwd16x16x32", "fwd8_c64", "fwd16_c64"]
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per launch from the committed ncu summary, keyed by workload."""
+    p = os.path.join(ROOT, "profiles", "dram_traffic.txt")
+    out = {}
+    if os.path.exists(p):
+        for line in open(p):
+            line = line.split("#")[0].split()
+            if len(line) >= 2:
+                try:
+                    out[line[0]] = float(line[1])
+                except ValueError:
+                    pass
+    return out
+
+
+def field(rng, shape, dist, dtype):
+    if dist == "uniform":
+        x = rng.uniform(-1.0, 1.0, shape) + 1j * rng.uniform(-1.0, 1.0, shape)
+    else:
+        x = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    return x.astype(dtype)
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200", "-f", self.path],
+                stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [c.strip() for c in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx.append(float(f[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, f[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+            os.unlink(self.path)
+        except Exception:
+            pass
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+# ------------------------------------------------------------------ device timing
+
+class Workload:
+    """Plans and device buffers for one workload on this rank's GPU."""
+
+    def __init__(self, fb, torch, name, device, seed):
+        w = WORKLOADS[name]
+        self.name, self.w = name, w
+        self.torch, self.fb = torch, fb
+        self.shape, self.batch, self.prec = w["shape"], w["batch"], w["prec"]
+        self.plans = [fb.Plan(self.shape, self.batch, d, self.prec) for d in w["chain"]]
+        ndt = np.complex128 if self.prec == 0 else np.complex64
+        tdt = torch.complex128 if self.prec == 0 else torch.complex64
+        self.eb = 16 if self.prec == 0 else 8
+        self.vol = int(np.prod(self.shape))
+        self.bytes = self.batch * self.vol * self.eb
+        rng = np.random.default_rng(seed)
+        self.host = field(rng, (self.batch,) + self.shape, w["dist"], ndt)
+        # rotate buffer sets so every launch reads data that is not L2-resident
+        per_set = self.bytes * (len(w["chain"]) + 1)
+        self.nsets = max(1, -(-3 * L2_BYTES // per_set))
+        x = torch.from_numpy(self.host).to(device)
+        self.sets = []
+        for k in range(self.nsets):
+            bufs = [x if k == 0 else x.clone()]
+            for _ in w["chain"]:
+                bufs.append(torch.empty_like(x))
+            self.sets.append(bufs)
+        self.tdt = tdt
+        self.it = 0
+
+    def step(self, stream, ev=None):
+        bufs = self.sets[self.it % self.nsets]
+        self.it += 1
+        for k, p in enumerate(self.plans):
+            if ev is not None and k == 0:
+                ev[0].record(stream)
+            p.execute(bufs[k].data_ptr(), bufs[k + 1].data_ptr(), stream.cuda_stream)
+            if ev is not None and k == 0:
+                ev[1].record(stream)
+
+    def launches_per_step(self):
+        return sum(p.launches() for p in self.plans)
+
+
+def time_device(torch, wl, stream, steps, warmup, dist=None, sampler=None):
+    for _ in range(warmup):
+        wl.step(stream)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    if sampler:
+        sampler.start()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(steps)]
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for k in range(steps):
+        wl.step(stream, evs[k])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop() if sampler else None
+    total_ms = e0.elapsed_time(e1)
+    first_ms = [a.elapsed_time(b) for a, b in evs]
+    if dist is not None:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=stream.device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    return total_ms / steps, statistics.mean(first_ms), clocks
+
+
+def time_e2e(fb, torch, wl, steps, warmup, dist=None):
+    """Whole step through the host-pointer C ABI, page-locked buffers."""
+    pin_in = torch.from_numpy(wl.host).pin_memory()
+    pin_out = torch.empty_like(pin_in).pin_memory()
+    lib = fb.lib()
+    arr = (ctypes.c_void_p * len(wl.plans))(*[p.handle.value for p in wl.plans])
+    for _ in range(warmup):
+        st = lib.fft3d_b200_execute_host_chain(arr, len(wl.plans), pin_in.data_ptr(),
+                                               pin_out.data_ptr())
+        if st != 0:
+            raise fb.Fft3dError(st, "execute_host_chain")
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        lib.fft3d_b200_execute_host_chain(arr, len(wl.plans), pin_in.data_ptr(),
+                                          pin_out.data_ptr())
+        _ = pin_out[0, 0, 0, 0].item()  # the step's result is read on the host
+    dt = (time.perf_counter() - t0) / steps
+    if dist is not None:
+        t = torch.tensor([dt], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dt = float(t.item())
+    return dt, wl.bytes, wl.bytes
+
+
+# ------------------------------------------------------------------ CPU reference
+
+def aligned(shape, dtype=np.complex128, align=64):
+    n = int(np.prod(shape)) * np.dtype(dtype).itemsize
+    buf = np.empty(n + align, dtype=np.uint8)
+    off = (-buf.ctypes.data) % align
+    return buf[off:off + n].view(dtype).reshape(shape)
+
+
+def cpu_reference(name, seconds=10.0, threads=None, max_sample=None):
+    """The reference's own C kernels (oracle/_ref) when built, else the oracle port.
+    Returns (volumes/s, kind, threads, sample description, per-run seconds)."""
+    w = WORKLOADS[name]
+    L = w["shape"][0]
+    roundtrip = len(w["chain"]) == 2
+    threads = threads or os.cpu_count() or 1
+    lib_path = os.path.join(ROOT, "oracle", "_ref", "libfft3d_best.so")
+    vol = int(np.prod(w["shape"]))
+    sample = max_sample or max(threads * 4, min(w["batch"], (64 << 20) // (vol * 16)))
+    sample = min(sample, w["batch"])
+    rng = np.random.default_rng(99)
+    x = aligned((sample,) + w["shape"])
+    x[:] = field(rng, (sample,) + w["shape"], w["dist"], np.complex128)
+    out = aligned((sample,) + w["shape"])
+    if os.path.exists(lib_path) and w["prec"] == 0 and w["shape"][0] == w["shape"][1] == w["shape"][2]:
+        lib = ctypes.CDLL(lib_path)
+        lib.ref_create.restype = ctypes.c_void_p
+        lib.ref_create.argtypes = [ctypes.c_int, ctypes.c_long, ctypes.c_int, ctypes.c_int]
+        lib.ref_run.argtypes = [ctypes.c_void_p] * 3
+        lib.ref_destroy.argtypes = [ctypes.c_void_p]
+        lib.ref_kernel_name.argtypes = [ctypes.c_void_p]
+        lib.ref_kernel_name.restype = ctypes.c_char_p
+        ctx = lib.ref_create(L, sample, threads, 1 if roundtrip else 0)
+        run = lambda: lib.ref_run(ctx, x.ctypes.data, out.ctypes.data)  # noqa: E731
+        kind = "reference"
+        kname = lib.ref_kernel_name(ctx).decode()
+        desc = (f"bench/geom/best {kname} (reference C, -march=sapphirerapids), "
+                f"{sample} volumes per run{', inverse by conjugation' if roundtrip else ''}")
+    else:
+        import oracle
+        ctx = None
+
+        def run():
+            y = oracle.fft3d(x, nthreads=threads)
+            if roundtrip:
+                oracle.ifft3d(y, nthreads=threads)
+        kind = "port"
+        desc = f"oracle/fft3d_oracle.c restatement, {sample} volumes per run"
+    run()  # first touch
+    runs, t0 = 0, time.perf_counter()
+    while True:
+        run()
+        runs += 1
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    per = el / runs
+    if ctx:
+        lib.ref_destroy(ctx)
+    return sample / per, kind, threads, desc + f", {runs} runs over {el:.1f} s", per
+
+
+# ------------------------------------------------------------------ main
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="roundtrip17", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-extra", action="store_true", help="skip the per-L workloads")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    a = ap.parse_args()
+    a.warmup = max(a.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    w = WORKLOADS[a.workload]
+    metric = f"volumes/s ({w['label']})"
+
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        vps = []
+        per_step = None
+        for _ in range(a.warmup):
+            cpu_reference(a.workload, seconds=0.0)
+        for _ in range(a.steps):
+            v, kind, thr, desc, per_step = cpu_reference(a.workload, seconds=0.0)
+            vps.append(v)
+        value = statistics.median(vps)
+        line = {"impl": "reference", "metric": metric, "value": value, "unit": "volumes/s",
+                "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+                "ms_per_step": per_step * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": a.workload, "shape": list(w["shape"]),
+                           "global_batch": w["batch"], "precision": "c128",
+                           "step": "forward+inverse" if len(w["chain"]) == 2 else "forward"},
+                "cpu_baseline": {"value": value, "unit": "volumes/s", "cores": thr, "kind": kind,
+                                 "sample": desc},
+                "e2e": {"value": value, "unit": "volumes/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    import fft3d_b200 as fb
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as tdist
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    else:
+        torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=device)
+    peak, peak_kind = peaks()
+    traffic = ncu_traffic()
+
+    wl = Workload(fb, torch, a.workload, device, seed=1234 + rank)
+    sampler = ClockSampler(local)
+    ms, first_ms, clocks = time_device(torch, wl, stream, a.steps, a.warmup, dist, sampler)
+    value = world * wl.batch / (ms * 1e-3)
+    alg_bytes = 2 * wl.bytes
+    achieved = alg_bytes / (first_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
+                "kernel": wl.plans[0].describe(),
+                "alg_bytes_per_launch": alg_bytes,
+                "traffic": traffic.get(a.workload.replace("roundtrip", "fwd")),
+                "ms_per_launch": first_ms}
+
+    e2e_s, h2d, d2h = time_e2e(fb, torch, wl, max(3, a.steps // 2), 2, dist)
+    e2e = {"value": world * wl.batch / e2e_s, "unit": "volumes/s", "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": d2h,
+           "path": "fft3d_b200_execute_host_chain, page-locked host buffers"}
+
+    workloads = {}
+    if not a.no_extra:
+        for name in EXTRA:
+            ww = WORKLOADS[name]
+            if not fb.supports(ww["shape"], ww["prec"]):
+                workloads[name] = {"supported": False}
+                continue
+            x = Workload(fb, torch, name, device, seed=77)
+            m, f, _ = time_device(torch, x, stream, max(5, a.steps // 2), a.warmup, dist, None)
+            ab = 2 * x.bytes
+            ach = ab / (f * 1e-3) / 1e9
+            workloads[name] = {"label": ww["label"], "volumes_per_s": world * x.batch / (m * 1e-3),
+                               "ms_per_launch": f, "achieved_gbs": ach, "frac": ach / peak,
+                               "kernel": x.plans[0].describe(),
+                               "traffic": traffic.get(name)}
+            del x
+            torch.cuda.empty_cache()
+
+    cpu = None
+    if rank == 0 and world == 1:
+        v, kind, thr, desc, _ = cpu_reference(a.workload, seconds=a.cpu_seconds)
+        cpu = {"value": v, "unit": "volumes/s", "cores": thr, "kind": kind, "sample": desc}
+
+    line = {"metric": metric, "value": value, "unit": "volumes/s", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": a.workload, "shape": list(w["shape"]),
+                       "global_batch": world * w["batch"], "per_gpu_batch": w["batch"],
+                       "precision": "c128" if w["prec"] == 0 else "c64",
+                       "step": "forward+inverse" if len(w["chain"]) == 2 else "forward",
+                       "l2": (f"inputs larger than L2 ({wl.bytes / 2**20:.0f} MiB per buffer, "
+                              f"{wl.nsets} rotating buffer sets)"),
+                       "parallelism": f"dp{world} (volumes sharded, no collective)"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "clocks": clocks, "gpu_launches": a.steps * wl.launches_per_step(),
+            "workloads": workloads}
+    if rank == 0:
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,140 @@
+/* fft3d_b200.h -- extension API of the B200 batched 3D complex FFT.
+ *
+ * The six symbols of the reference contract are unchanged and live in
+ * fft3d_api.h (host pointers) and fft3d_gpu_api.h (device pointers).  This header
+ * adds what that contract cannot express (SURVEY of the reference: forward-only,
+ * cubes only, complex double only, void returns):
+ *
+ *   - anisotropic n0 x n1 x n2 extents       (python/fft3d.py:360-371 handles any shape)
+ *   - direction: forward, or backward with 1/V (python/fft3d.py:402-423)
+ *   - precision: complex128, complex64 in FP32 (python/fft3d.py:368-371 keeps c64 I/O)
+ *   - status-returning execute on a caller stream, and host-pointer execute
+ *   - descriptor-list batches of uneven geometry run by one persistent launch
+ *
+ * Layout everywhere: element (b, i0, i1, i2) at ((b*n0 + i0)*n1 + i1)*n2 + i2,
+ * interleaved complex, batch slowest (bench/geom/fft3d_api.h:14-18).
+ * All transforms are out-of-place; `in` is never written.
+ */
+#ifndef FFT3D_B200_H
+#define FFT3D_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  0 is success; every failure is negative. */
+#define FFT3D_B200_OK 0
+#define FFT3D_B200_ERR_INVALID (-1)     /* null pointer, non-positive extent, bad enum */
+#define FFT3D_B200_ERR_UNSUPPORTED (-2) /* geometry / precision this build has no kernel for */
+#define FFT3D_B200_ERR_ALIGN (-3)       /* buffer not aligned to its element size */
+#define FFT3D_B200_ERR_CUDA (-4)        /* a CUDA runtime call failed (fault, launch error) */
+#define FFT3D_B200_ERR_NOMEM (-5)       /* device or pinned-host allocation failed */
+#define FFT3D_B200_ERR_TIMEOUT (-6)     /* a bounded device-side wait ran out */
+#define FFT3D_B200_ERR_BUDGET (-7)      /* request larger than the admission budget */
+#define FFT3D_B200_ERR_OVERLAP (-8)     /* in and out overlap; transforms are out-of-place */
+#define FFT3D_B200_ERR_BUSY (-9)        /* server queue full; retry later */
+
+#define FFT3D_B200_FORWARD (-1)  /* exp(-2*pi*i k.j/n), unnormalised */
+#define FFT3D_B200_BACKWARD (+1) /* exp(+2*pi*i k.j/n), scaled by 1/(n0*n1*n2) */
+
+#define FFT3D_B200_C128 0 /* complex double in, complex double out, FP64 arithmetic */
+#define FFT3D_B200_C64 1  /* complex float in and out, FP32 arithmetic */
+
+/* Plan flags. */
+#define FFT3D_B200_FLAG_NO_TUNE 0x1u   /* take the default kernel instead of timing candidates */
+#define FFT3D_B200_FLAG_NO_GRAPH 0x2u  /* batches: launch directly instead of replaying a CUDA graph */
+
+typedef struct fft3d_b200_plan fft3d_b200_plan;
+
+typedef struct {
+    int n0, n1, n2;      /* extents; n2 is the fastest-varying axis */
+    long long batch;     /* number of volumes, >= 0 */
+    int direction;       /* FFT3D_B200_FORWARD or FFT3D_B200_BACKWARD */
+    int precision;       /* FFT3D_B200_C128 or FFT3D_B200_C64 */
+    unsigned flags;      /* FFT3D_B200_FLAG_* */
+    int device;          /* CUDA device ordinal; -1 = the current device */
+} fft3d_b200_desc;
+
+/* Nonzero when this build has a kernel for the geometry and precision. */
+int fft3d_b200_supports(int n0, int n1, int n2, int precision);
+
+/* Create a plan: twiddle and Rader tables, kernel choice (timed candidates unless
+ * FFT3D_B200_FLAG_NO_TUNE), staging for host-pointer execution.  Returns a status;
+ * *out is NULL on failure. */
+int fft3d_b200_plan_create(const fft3d_b200_desc *desc, fft3d_b200_plan **out);
+
+void fft3d_b200_plan_destroy(fft3d_b200_plan *plan);
+
+/* Transform device-resident data on `stream` (a cudaStream_t; NULL = the legacy
+ * default stream).  Asynchronous: returns once the work is enqueued.  `in` and
+ * `out` must be distinct device buffers of batch*n0*n1*n2 elements aligned to the
+ * element size. */
+int fft3d_b200_execute(fft3d_b200_plan *plan, const void *d_in, void *d_out, void *stream);
+
+/* Transform host data: copies in, transforms, copies out, and returns when `out`
+ * holds the result.  Page-locked buffers are transferred directly; pageable ones
+ * through the plan's pinned staging, in overlapped chunks. */
+int fft3d_b200_execute_host(fft3d_b200_plan *plan, const void *h_in, void *h_out);
+
+/* Run plans[0], plans[1], ... back to back on the device between ONE host-to-device
+ * copy of h_in and ONE device-to-host copy into h_out (e.g. a forward and a
+ * backward plan for a round trip).  All plans must have the same geometry,
+ * precision and batch. */
+int fft3d_b200_execute_host_chain(fft3d_b200_plan *const *plans, int nplans, const void *h_in,
+                                  void *h_out);
+
+/* Names of the compiled kernel variants for a geometry, precision and direction
+ * (the autotuner's candidates).  Writes up to `max` names and returns the count. */
+int fft3d_b200_variants(int n0, int n1, int n2, int precision, int direction, const char **names,
+                        int max);
+
+/* Like fft3d_b200_plan_create, but use the named variant instead of tuning. */
+int fft3d_b200_plan_create_variant(const fft3d_b200_desc *desc, const char *variant,
+                                   fft3d_b200_plan **out);
+
+/* Human-readable description of the kernel configuration the plan selected. */
+const char *fft3d_b200_plan_describe(const fft3d_b200_plan *plan);
+
+/* Number of kernel launches one execute of this plan issues. */
+int fft3d_b200_plan_launches(const fft3d_b200_plan *plan);
+
+/* Status of the most recent call into the reference-contract entry points
+ * (fft3d_execute / fft3d_gpu_execute return void) on this host thread. */
+int fft3d_b200_last_status(void);
+
+const char *fft3d_b200_status_string(int status);
+
+/* ---------------------------------------------------------------- batches of uneven geometry */
+
+typedef struct {
+    int n0, n1, n2;      /* extents of every volume of the segment */
+    int direction;       /* FFT3D_B200_FORWARD / FFT3D_B200_BACKWARD */
+    int precision;       /* FFT3D_B200_C128 / FFT3D_B200_C64 */
+    long long batch;     /* volumes in the segment */
+    const void *in;      /* device pointer */
+    void *out;           /* device pointer */
+} fft3d_b200_segment;
+
+typedef struct fft3d_b200_batch fft3d_b200_batch;
+
+/* Build a batch over `nseg` segments: validates them, uploads a descriptor list of
+ * work items to the device, tunes the persistent launch and, unless
+ * FFT3D_B200_FLAG_NO_GRAPH, captures it in a CUDA graph. */
+int fft3d_b200_batch_create(const fft3d_b200_segment *segs, int nseg, unsigned flags, int device,
+                            fft3d_b200_batch **out);
+
+/* Run every segment of the batch in one persistent launch on `stream`. */
+int fft3d_b200_batch_execute(fft3d_b200_batch *batch, void *stream);
+
+void fft3d_b200_batch_destroy(fft3d_b200_batch *batch);
+
+const char *fft3d_b200_batch_describe(const fft3d_b200_batch *batch);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FFT3D_B200_H */

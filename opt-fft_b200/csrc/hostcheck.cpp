@@ -1,0 +1,79 @@
+// hostcheck.cpp -- CPU execution of the kernels' pass code, for unit tests only.
+//
+// Test infrastructure: built into build/libfft3d_hostcheck.so, loaded only by
+// tests/, never linked into libfft3d_b200.so.  It runs the very functions the
+// VOLUME kernels run (stage_in, pass_z, pass_y, pass_x_out of volume.cuh, the
+// codelets of codelets.cuh, the layouts of Geom), one "thread" after another and
+// one CTA after another, so the index arithmetic, the shared-memory layouts and
+// every codelet are checked against the oracle without a GPU.
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "volume.cuh"
+
+namespace fft3d {
+void ensure_host_tables();
+}
+
+using namespace fft3d;
+
+template <int N0, int N1, int N2, typename T, int S, int ALG, int VPC>
+static void emulate(const void *vin, void *vout, long long nvol)
+{
+    using G = Geom<N0, N1, N2, T>;
+    const cx<T> *in = (const cx<T> *)vin;
+    cx<T> *out = (cx<T> *)vout;
+    std::vector<cx<T>> sm((size_t)VPC * G::PV);
+    const T scale = S > 0 ? T(1) / T(G::V) : T(1);
+    for (long long v0 = 0; v0 < nvol; v0 += VPC) {
+        const int nv = (int)((nvol - v0) < VPC ? (nvol - v0) : VPC);
+        // poison the layout so a slot the kernels never write would show up
+        for (auto &e : sm) e = {T(12345.0), T(-6789.0)};
+        for (int g = 0; g < nv * G::V; ++g) stage_in<G>(sm.data(), in + v0 * G::V, g);
+        for (int r = 0; r < nv * G::ROWS; ++r) pass_z<G, S, ALG>(sm.data(), r);
+        for (int l = 0; l < nv * G::N0 * G::N2; ++l) pass_y<G, S, ALG>(sm.data(), l);
+        for (int l = 0; l < nv * G::N1 * G::N2; ++l)
+            pass_x_out<G, S, ALG>(sm.data(), l, out + v0 * G::V, scale);
+    }
+}
+
+typedef void (*emu_fn)(const void *, void *, long long);
+
+struct EmuEntry {
+    int n0, n1, n2, prec, sign, alg, vpc;
+    emu_fn fn;
+};
+
+#define EMU(N0, N1, N2, T, ALG, VPC)                                                           \
+    {N0, N1, N2, sizeof(T) == 8 ? 0 : 1, -1, ALG, VPC, &emulate<N0, N1, N2, T, -1, ALG, VPC>}, \
+    {N0, N1, N2, sizeof(T) == 8 ? 0 : 1, +1, ALG, VPC, &emulate<N0, N1, N2, T, +1, ALG, VPC>}
+
+static const EmuEntry kEmu[] = {
+    EMU(6, 6, 6, double, 0, 16),   EMU(8, 8, 8, double, 0, 8),     EMU(12, 12, 12, double, 0, 2),
+    EMU(16, 16, 16, double, 0, 1), EMU(17, 17, 17, double, 0, 1),  EMU(17, 17, 17, double, 1, 1),
+    EMU(24, 24, 24, double, 0, 1), EMU(8, 8, 16, double, 0, 8),    EMU(16, 16, 32, double, 0, 1),
+    EMU(36, 36, 36, double, 0, 1), EMU(6, 6, 6, float, 0, 32),     EMU(8, 8, 8, float, 0, 16),
+    EMU(12, 12, 12, float, 0, 4),  EMU(16, 16, 16, float, 0, 2),   EMU(17, 17, 17, float, 0, 2),
+    EMU(17, 17, 17, float, 1, 2),  EMU(24, 24, 24, float, 0, 1),   EMU(8, 8, 16, float, 0, 16),
+    EMU(16, 16, 32, float, 0, 1),  EMU(36, 36, 36, float, 0, 1),   EMU(2, 3, 5, double, 0, 3),
+    EMU(7, 11, 13, double, 0, 2),  EMU(9, 9, 9, double, 0, 2),     EMU(5, 8, 12, double, 0, 1),
+    EMU(32, 8, 4, double, 0, 1),   EMU(13, 5, 8, double, 0, 1),    EMU(4, 4, 4, double, 0, 2),
+    EMU(1, 8, 8, double, 0, 1),    EMU(8, 1, 8, double, 0, 1),     EMU(8, 8, 1, double, 0, 1),
+    EMU(1, 1, 1, double, 0, 1),    EMU(3, 3, 3, double, 0, 1),     EMU(17, 2, 2, double, 0, 1),
+};
+
+extern "C" int hostcheck_fft3d(int n0, int n1, int n2, int prec, int sign, int alg, int vpc,
+                               const void *in, void *out, long long nvol)
+{
+    ensure_host_tables();
+    for (const auto &e : kEmu) {
+        if (e.n0 == n0 && e.n1 == n1 && e.n2 == n2 && e.prec == prec && e.sign == sign &&
+            e.alg == alg && (vpc <= 0 || e.vpc == vpc)) {
+            e.fn(in, out, nvol);
+            return 0;
+        }
+    }
+    return -2;
+}

@@ -1,0 +1,662 @@
+// plan.cu -- plans, the autotuner, host-pointer staging and every exported symbol.
+//
+// Exports the reference contract twice -- host pointers (bench/geom/fft3d_api.h:49-66)
+// and device pointers (bench/gpu/fft3d_gpu_api.h:57-83) -- and the extension API
+// of fft3d_b200.h.  All precomputation happens at plan creation
+// (bench/geom/fft3d_api.h:30-32): tables, kernel choice by timing the compiled
+// variants (the plan-time race of bench/geom/best/fft3d_best.c:131-193, done on
+// the GPU over kernel variants), device buffers and pinned staging.  There is no
+// CPU fallback: without a usable CUDA device every create fails.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <tuple>
+#include <vector>
+
+#include "../../include/fft3d_api.h"
+#include "../../include/fft3d_b200.h"
+#include "../../include/fft3d_gpu_api.h"
+#include "internal.h"
+
+namespace fft3d {
+
+static thread_local int t_last_status = FFT3D_B200_OK;
+
+static int set_status(int s)
+{
+    t_last_status = s;
+    return s;
+}
+
+int element_bytes(int precision) { return precision == FFT3D_B200_C64 ? 8 : 16; }
+
+const std::vector<KernelEntry> &registry()
+{
+    static std::vector<KernelEntry> reg;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        register_kernels(reg);
+        register_cluster_kernels(reg);
+    });
+    return reg;
+}
+
+cudaError_t launch_entry(const KernelEntry &e, const void *in, void *out, long long nvol,
+                         double scale, cudaStream_t stream, int num_sms)
+{
+    (void)num_sms;
+    if (nvol <= 0) return cudaSuccess;
+    if (e.family == FAM_VOLUME) {
+        const long long grid = (nvol + e.vpc - 1) / e.vpc;
+        if (grid > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+        if (e.precision == FFT3D_B200_C128) {
+            double s = scale;
+            void *args[] = {(void *)&in, (void *)&out, (void *)&nvol, (void *)&s};
+            return cudaLaunchKernel(e.func, dim3((unsigned)grid), dim3(e.threads), args,
+                                    (size_t)e.smem, stream);
+        } else {
+            float s = (float)scale;
+            void *args[] = {(void *)&in, (void *)&out, (void *)&nvol, (void *)&s};
+            return cudaLaunchKernel(e.func, dim3((unsigned)grid), dim3(e.threads), args,
+                                    (size_t)e.smem, stream);
+        }
+    }
+    if (e.family == FAM_CLUSTER) {
+        // one cluster of e.vpc CTAs per volume
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(nvol * e.vpc));
+        cfg.blockDim = dim3(e.threads);
+        cfg.dynamicSmemBytes = (size_t)e.smem;
+        cfg.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = e.vpc;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        if (e.precision == FFT3D_B200_C128) {
+            double s = scale;
+            void *args[] = {(void *)&in, (void *)&out, (void *)&nvol, (void *)&s};
+            return cudaLaunchKernelExC(&cfg, e.func, args);
+        } else {
+            float s = (float)scale;
+            void *args[] = {(void *)&in, (void *)&out, (void *)&nvol, (void *)&s};
+            return cudaLaunchKernelExC(&cfg, e.func, args);
+        }
+    }
+    return cudaErrorInvalidValue;
+}
+
+// Per-device attribute setup of a kernel (dynamic shared memory above 48 KB).
+static int prepare_entry(const KernelEntry &e, int device)
+{
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, bool> done;
+    std::lock_guard<std::mutex> lk(mu);
+    auto key = std::make_pair(e.func, device);
+    if (done.count(key)) return FFT3D_B200_OK;
+    if (cudaFuncSetAttribute(e.func, cudaFuncAttributeMaxDynamicSharedMemorySize, e.smem) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return FFT3D_B200_ERR_UNSUPPORTED;
+    }
+    if (e.family == FAM_CLUSTER) {
+        if (cudaFuncSetAttribute(e.func, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+            cudaSuccess)
+            cudaGetLastError();
+    }
+    done[key] = true;
+    return FFT3D_B200_OK;
+}
+
+static std::vector<const KernelEntry *> candidates(int n0, int n1, int n2, int precision, int sign)
+{
+    std::vector<const KernelEntry *> c;
+    for (const auto &e : registry())
+        if (e.n0 == n0 && e.n1 == n1 && e.n2 == n2 && e.precision == precision && e.sign == sign)
+            c.push_back(&e);
+    return c;
+}
+
+// Process-wide memo of tuning results: (device, geometry, precision, sign, batch
+// bucket) -> registry index of the winner.
+static std::mutex g_tune_mu;
+static std::map<std::tuple<int, int, int, int, int, int, int>, const KernelEntry *> g_tuned;
+
+static int batch_bucket(long long b)
+{
+    int k = 0;
+    while (b > 1 && k < 62) { b >>= 1; ++k; }
+    return k;
+}
+
+// Time every candidate on plan-owned scratch of min(batch, cap) volumes and
+// return the fastest.  Candidates that fail to launch are skipped.
+static const KernelEntry *tune(const std::vector<const KernelEntry *> &cands, int device,
+                               long long batch, int precision, long long vol_elems, int num_sms,
+                               std::string *log)
+{
+    if (cands.size() == 1) return cands[0];
+    const size_t eb = (size_t)element_bytes(precision);
+    long long cap = (long long)((size_t)512 << 20) / (long long)(vol_elems * eb);
+    if (cap < 1) cap = 1;
+    const long long nb = std::max(1LL, std::min(batch, cap));
+    const size_t bytes = (size_t)nb * vol_elems * eb;
+    void *a = nullptr, *b = nullptr;
+    if (cudaMalloc(&a, bytes) != cudaSuccess || cudaMalloc(&b, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        if (a) cudaFree(a);
+        return cands[0];
+    }
+    cudaMemset(a, 0x3f, bytes);  // finite, normal values in both precisions
+    cudaStream_t s;
+    cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const KernelEntry *best = nullptr;
+    float best_ms = 1e30f;
+    for (const KernelEntry *k : cands) {
+        if (prepare_entry(*k, device) != FFT3D_B200_OK) continue;
+        bool ok = true;
+        for (int w = 0; w < 2 && ok; ++w)
+            ok = launch_entry(*k, a, b, nb, 1.0, s, num_sms) == cudaSuccess;
+        if (!ok || cudaStreamSynchronize(s) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        float ms_min = 1e30f;
+        for (int rep = 0; rep < 3; ++rep) {
+            cudaEventRecord(e0, s);
+            for (int it = 0; it < 3; ++it) launch_entry(*k, a, b, nb, 1.0, s, num_sms);
+            cudaEventRecord(e1, s);
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            ms_min = std::min(ms_min, ms / 3.f);
+        }
+        if (log) {
+            char buf[256];
+            snprintf(buf, sizeof buf, "%s: %.3f us; ", k->name, ms_min * 1e3f);
+            *log += buf;
+        }
+        if (ms_min < best_ms) {
+            best_ms = ms_min;
+            best = k;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(s);
+    cudaFree(a);
+    cudaFree(b);
+    return best ? best : cands[0];
+}
+
+}  // namespace fft3d
+
+using namespace fft3d;
+
+struct fft3d_b200_plan {
+    fft3d_b200_desc desc;
+    int device;
+    int num_sms;
+    long long vol_elems;
+    size_t bytes;  // whole batch, one buffer
+    double scale;
+    const KernelEntry *kernel;
+    std::string describe;
+    // host-pointer execution
+    void *d_in = nullptr, *d_out = nullptr;
+    void *pin[2] = {nullptr, nullptr};
+    size_t pin_bytes = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t xs[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+};
+
+static int validate_desc(const fft3d_b200_desc *d)
+{
+    if (!d) return FFT3D_B200_ERR_INVALID;
+    if (d->n0 < 1 || d->n1 < 1 || d->n2 < 1 || d->batch < 0) return FFT3D_B200_ERR_INVALID;
+    if (d->direction != FFT3D_B200_FORWARD && d->direction != FFT3D_B200_BACKWARD)
+        return FFT3D_B200_ERR_INVALID;
+    if (d->precision != FFT3D_B200_C128 && d->precision != FFT3D_B200_C64)
+        return FFT3D_B200_ERR_INVALID;
+    return FFT3D_B200_OK;
+}
+
+extern "C" int fft3d_b200_supports(int n0, int n1, int n2, int precision)
+{
+    if (n0 < 1 || n1 < 1 || n2 < 1) return 0;
+    return candidates(n0, n1, n2, precision, -1).empty() ? 0 : 1;
+}
+
+extern "C" int fft3d_b200_variants(int n0, int n1, int n2, int precision, int direction,
+                                   const char **names, int max)
+{
+    auto c = candidates(n0, n1, n2, precision, direction);
+    for (int i = 0; i < (int)c.size() && i < max && names; ++i) names[i] = c[i]->name;
+    return (int)c.size();
+}
+
+static int plan_create_impl(const fft3d_b200_desc *desc, const char *variant,
+                            fft3d_b200_plan **out)
+{
+    if (!out) return set_status(FFT3D_B200_ERR_INVALID);
+    *out = nullptr;
+    int st = validate_desc(desc);
+    if (st) return set_status(st);
+    auto cands = candidates(desc->n0, desc->n1, desc->n2, desc->precision, desc->direction);
+    if (cands.empty()) return set_status(FFT3D_B200_ERR_UNSUPPORTED);
+    const KernelEntry *forced = nullptr;
+    if (variant) {
+        for (const KernelEntry *c : cands)
+            if (strcmp(c->name, variant) == 0) forced = c;
+        if (!forced) return set_status(FFT3D_B200_ERR_UNSUPPORTED);
+    }
+
+    int device = desc->device;
+    if (device < 0) {
+        if (cudaGetDevice(&device) != cudaSuccess) {
+            cudaGetLastError();
+            return set_status(FFT3D_B200_ERR_CUDA);
+        }
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device >= ndev) {
+        cudaGetLastError();
+        return set_status(FFT3D_B200_ERR_CUDA);
+    }
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (cudaSetDevice(device) != cudaSuccess) return set_status(FFT3D_B200_ERR_CUDA);
+    st = ensure_device_tables(device);
+    if (st) {
+        if (prev >= 0) cudaSetDevice(prev);
+        return set_status(st);
+    }
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+
+    fft3d_b200_plan *p = new fft3d_b200_plan();
+    p->desc = *desc;
+    p->device = device;
+    p->num_sms = sms;
+    p->vol_elems = (long long)desc->n0 * desc->n1 * desc->n2;
+    p->bytes = (size_t)desc->batch * (size_t)p->vol_elems * (size_t)element_bytes(desc->precision);
+    p->scale = desc->direction == FFT3D_B200_BACKWARD ? 1.0 / (double)p->vol_elems : 1.0;
+
+    const bool no_tune = (desc->flags & FFT3D_B200_FLAG_NO_TUNE) || getenv("FFT3D_B200_NO_TUNE");
+    const KernelEntry *k = forced;
+    if (!k) {
+        auto key = std::make_tuple(device, desc->n0, desc->n1, desc->n2, desc->precision,
+                                   desc->direction, batch_bucket(desc->batch));
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tuned.find(key);
+        if (it != g_tuned.end()) {
+            k = it->second;
+        } else if (!no_tune && desc->batch > 0) {
+            std::string log;
+            k = tune(cands, device, desc->batch, desc->precision, p->vol_elems, sms, &log);
+            g_tuned[key] = k;
+            if (getenv("FFT3D_B200_TUNE_LOG")) fprintf(stderr, "fft3d_b200 tune: %s\n", log.c_str());
+        }
+    }
+    if (!k) k = cands[0];
+    if (prepare_entry(*k, device) != FFT3D_B200_OK) {
+        delete p;
+        if (prev >= 0) cudaSetDevice(prev);
+        return set_status(FFT3D_B200_ERR_UNSUPPORTED);
+    }
+    p->kernel = k;
+    p->describe = k->name;
+    if (prev >= 0 && prev != device) cudaSetDevice(prev);
+    *out = p;
+    return set_status(FFT3D_B200_OK);
+}
+
+extern "C" int fft3d_b200_plan_create(const fft3d_b200_desc *desc, fft3d_b200_plan **out)
+{
+    return plan_create_impl(desc, nullptr, out);
+}
+
+extern "C" int fft3d_b200_plan_create_variant(const fft3d_b200_desc *desc, const char *variant,
+                                              fft3d_b200_plan **out)
+{
+    if (!variant) return set_status(FFT3D_B200_ERR_INVALID);
+    return plan_create_impl(desc, variant, out);
+}
+
+static void free_staging(fft3d_b200_plan *p)
+{
+    if (p->d_in) cudaFree(p->d_in);
+    if (p->d_out) cudaFree(p->d_out);
+    for (int i = 0; i < 2; ++i) {
+        if (p->pin[i]) cudaFreeHost(p->pin[i]);
+        if (p->xs[i]) cudaStreamDestroy(p->xs[i]);
+        if (p->ev[i]) cudaEventDestroy(p->ev[i]);
+        p->pin[i] = nullptr;
+        p->xs[i] = nullptr;
+        p->ev[i] = nullptr;
+    }
+    if (p->stream) cudaStreamDestroy(p->stream);
+    p->d_in = p->d_out = nullptr;
+    p->stream = nullptr;
+}
+
+extern "C" void fft3d_b200_plan_destroy(fft3d_b200_plan *p)
+{
+    if (!p) return;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(p->device);
+    cudaDeviceSynchronize();
+    free_staging(p);
+    if (prev >= 0) cudaSetDevice(prev);
+    delete p;
+}
+
+static bool ranges_overlap(const void *a, const void *b, size_t n)
+{
+    const char *x = (const char *)a, *y = (const char *)b;
+    return x < y + n && y < x + n;
+}
+
+extern "C" int fft3d_b200_execute(fft3d_b200_plan *p, const void *d_in, void *d_out, void *stream)
+{
+    if (!p) return set_status(FFT3D_B200_ERR_INVALID);
+    if (p->desc.batch == 0) return set_status(FFT3D_B200_OK);
+    if (!d_in || !d_out) return set_status(FFT3D_B200_ERR_INVALID);
+    const uintptr_t al = (uintptr_t)element_bytes(p->desc.precision);
+    if (((uintptr_t)d_in % al) || ((uintptr_t)d_out % al)) return set_status(FFT3D_B200_ERR_ALIGN);
+    if (ranges_overlap(d_in, d_out, p->bytes)) return set_status(FFT3D_B200_ERR_OVERLAP);
+    cudaError_t e = launch_entry(*p->kernel, d_in, d_out, p->desc.batch, p->scale,
+                                 (cudaStream_t)stream, p->num_sms);
+    if (e != cudaSuccess) return set_status(FFT3D_B200_ERR_CUDA);
+    return set_status(FFT3D_B200_OK);
+}
+
+// ------------------------------------------------------------------ host-pointer execution
+
+static int ensure_staging(fft3d_b200_plan *p)
+{
+    if (p->d_in) return FFT3D_B200_OK;
+    const size_t eb = (size_t)element_bytes(p->desc.precision);
+    const size_t vb = (size_t)p->vol_elems * eb;
+    if (cudaMalloc(&p->d_in, p->bytes) != cudaSuccess || cudaMalloc(&p->d_out, p->bytes) != cudaSuccess) {
+        cudaGetLastError();
+        free_staging(p);
+        return FFT3D_B200_ERR_NOMEM;
+    }
+    // pinned staging chunks of ~8 MB (at least one volume)
+    size_t chunk = std::max(vb, ((size_t)8 << 20) / vb * vb);
+    chunk = std::min(chunk, p->bytes);
+    p->pin_bytes = chunk;
+    for (int i = 0; i < 2; ++i) {
+        if (cudaHostAlloc(&p->pin[i], 2 * chunk, cudaHostAllocDefault) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&p->xs[i], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&p->ev[i], cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            free_staging(p);
+            return FFT3D_B200_ERR_NOMEM;
+        }
+    }
+    if (cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        free_staging(p);
+        return FFT3D_B200_ERR_NOMEM;
+    }
+    return FFT3D_B200_OK;
+}
+
+static bool is_pinned(const void *ptr)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, ptr) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+static void par_memcpy(void *dst, const void *src, size_t n)
+{
+    const size_t kMin = (size_t)4 << 20;
+    unsigned nt = std::thread::hardware_concurrency();
+    if (nt > 8) nt = 8;
+    if (n < kMin || nt < 2) {
+        memcpy(dst, src, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    const size_t per = (n + nt - 1) / nt;
+    for (unsigned t = 0; t < nt; ++t) {
+        const size_t o = (size_t)t * per;
+        if (o >= n) break;
+        const size_t len = std::min(per, n - o);
+        th.emplace_back([=] { memcpy((char *)dst + o, (const char *)src + o, len); });
+    }
+    for (auto &x : th) x.join();
+}
+
+// Run `nplans` transforms on device copies of the batch, chunk by chunk, between
+// one upload and one download.  Chunks alternate over two streams so the copy
+// engines, the kernels and (for pageable buffers) the host copies overlap.
+static int run_host_chain(fft3d_b200_plan *const *plans, int nplans, const void *h_in, void *h_out)
+{
+    fft3d_b200_plan *p = plans[0];
+    int st = ensure_staging(p);
+    if (st) return st;
+    const size_t eb = (size_t)element_bytes(p->desc.precision);
+    const size_t vb = (size_t)p->vol_elems * eb;
+    const bool pinned = is_pinned(h_in) && is_pinned(h_out);
+    const size_t chunk = p->pin_bytes;
+    const size_t nchunks = (p->bytes + chunk - 1) / chunk;
+    const char *src = (const char *)h_in;
+    char *dst = (char *)h_out;
+    cudaError_t err = cudaSuccess;
+    auto chunk_len = [&](size_t c) { return std::min(chunk, p->bytes - c * chunk); };
+    for (size_t c = 0; c < nchunks; ++c) {
+        const int slot = (int)(c & 1);
+        cudaStream_t s = p->xs[slot];
+        const size_t off = c * chunk, len = chunk_len(c);
+        const long long nv = (long long)(len / vb);
+        char *din = (char *)p->d_in + off;
+        char *dout = (char *)p->d_out + off;
+        char *stage_in = (char *)p->pin[slot];
+        char *stage_out = stage_in + chunk;
+        if (!pinned) {
+            // the slot's previous chunk must be downloaded and copied out first
+            if (c >= 2) {
+                if (cudaEventSynchronize(p->ev[slot]) != cudaSuccess) return FFT3D_B200_ERR_CUDA;
+                par_memcpy(dst + (c - 2) * chunk, stage_out, chunk_len(c - 2));
+            }
+            par_memcpy(stage_in, src + off, len);
+            err = cudaMemcpyAsync(din, stage_in, len, cudaMemcpyHostToDevice, s);
+        } else {
+            err = cudaMemcpyAsync(din, src + off, len, cudaMemcpyHostToDevice, s);
+        }
+        if (err != cudaSuccess) return FFT3D_B200_ERR_CUDA;
+        char *a = din, *b = dout;
+        for (int i = 0; i < nplans; ++i) {
+            err = launch_entry(*plans[i]->kernel, a, b, nv, plans[i]->scale, s, p->num_sms);
+            if (err != cudaSuccess) return FFT3D_B200_ERR_CUDA;
+            std::swap(a, b);
+        }
+        // result is in `a` after the swap
+        err = cudaMemcpyAsync(pinned ? dst + off : stage_out, a, len, cudaMemcpyDeviceToHost, s);
+        if (err != cudaSuccess) return FFT3D_B200_ERR_CUDA;
+        if (cudaEventRecord(p->ev[slot], s) != cudaSuccess) return FFT3D_B200_ERR_CUDA;
+    }
+    if (!pinned) {
+        for (size_t c = (nchunks >= 2 ? nchunks - 2 : 0); c < nchunks; ++c) {
+            const int slot = (int)(c & 1);
+            if (cudaEventSynchronize(p->ev[slot]) != cudaSuccess) return FFT3D_B200_ERR_CUDA;
+            par_memcpy(dst + c * chunk, (char *)p->pin[slot] + chunk, chunk_len(c));
+        }
+    }
+    for (int i = 0; i < 2; ++i)
+        if (cudaStreamSynchronize(p->xs[i]) != cudaSuccess) return FFT3D_B200_ERR_CUDA;
+    return FFT3D_B200_OK;
+}
+
+extern "C" int fft3d_b200_execute_host_chain(fft3d_b200_plan *const *plans, int nplans,
+                                             const void *h_in, void *h_out)
+{
+    if (!plans || nplans < 1 || !plans[0]) return set_status(FFT3D_B200_ERR_INVALID);
+    const fft3d_b200_plan *p0 = plans[0];
+    for (int i = 1; i < nplans; ++i) {
+        const fft3d_b200_plan *q = plans[i];
+        if (!q || q->desc.n0 != p0->desc.n0 || q->desc.n1 != p0->desc.n1 ||
+            q->desc.n2 != p0->desc.n2 || q->desc.precision != p0->desc.precision ||
+            q->desc.batch != p0->desc.batch || q->device != p0->device)
+            return set_status(FFT3D_B200_ERR_INVALID);
+    }
+    if (p0->desc.batch == 0) return set_status(FFT3D_B200_OK);
+    if (!h_in || !h_out) return set_status(FFT3D_B200_ERR_INVALID);
+    if (ranges_overlap(h_in, h_out, p0->bytes)) return set_status(FFT3D_B200_ERR_OVERLAP);
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != p0->device) cudaSetDevice(p0->device);
+    int st = run_host_chain(plans, nplans, h_in, h_out);
+    if (prev >= 0 && prev != p0->device) cudaSetDevice(prev);
+    return set_status(st);
+}
+
+extern "C" int fft3d_b200_execute_host(fft3d_b200_plan *p, const void *h_in, void *h_out)
+{
+    fft3d_b200_plan *const one[1] = {p};
+    return fft3d_b200_execute_host_chain(one, 1, h_in, h_out);
+}
+
+extern "C" const char *fft3d_b200_plan_describe(const fft3d_b200_plan *p)
+{
+    return p ? p->describe.c_str() : "";
+}
+
+extern "C" int fft3d_b200_plan_launches(const fft3d_b200_plan *p) { return p ? 1 : 0; }
+
+extern "C" int fft3d_b200_last_status(void) { return t_last_status; }
+
+extern "C" const char *fft3d_b200_status_string(int s)
+{
+    switch (s) {
+    case FFT3D_B200_OK: return "ok";
+    case FFT3D_B200_ERR_INVALID: return "invalid argument";
+    case FFT3D_B200_ERR_UNSUPPORTED: return "unsupported geometry or precision";
+    case FFT3D_B200_ERR_ALIGN: return "buffer not aligned to its element size";
+    case FFT3D_B200_ERR_CUDA: return "CUDA runtime error";
+    case FFT3D_B200_ERR_NOMEM: return "out of memory";
+    case FFT3D_B200_ERR_TIMEOUT: return "bounded device wait timed out";
+    case FFT3D_B200_ERR_BUDGET: return "request exceeds the admission budget";
+    case FFT3D_B200_ERR_OVERLAP: return "input and output overlap";
+    case FFT3D_B200_ERR_BUSY: return "queue full";
+    default: return "unknown status";
+    }
+}
+
+// ------------------------------------------------------------------ reference contract, host pointers
+
+struct fft3d_plan {
+    fft3d_b200_plan *p;
+};
+
+static const char kName[] = "b200_fft3d";
+static const char kDesc[] =
+    "B200 sm_100a: volumes staged once in CTA shared memory (clusters + DSMEM beyond it), "
+    "register codelets (PFA/CT/Rader-17), coalesced streaming stores";
+
+extern "C" const char *fft3d_name(void) { return kName; }
+extern "C" const char *fft3d_description(void) { return kDesc; }
+extern "C" int fft3d_supports(int L) { return fft3d_b200_supports(L, L, L, FFT3D_B200_C128); }
+
+extern "C" fft3d_plan *fft3d_create(int L, int batch)
+{
+    if (L < 1 || batch < 1) {
+        set_status(FFT3D_B200_ERR_INVALID);
+        return nullptr;
+    }
+    fft3d_b200_desc d = {L, L, L, batch, FFT3D_B200_FORWARD, FFT3D_B200_C128, 0u, -1};
+    fft3d_b200_plan *p = nullptr;
+    if (fft3d_b200_plan_create(&d, &p) != FFT3D_B200_OK) return nullptr;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(p->device);
+    const int st = ensure_staging(p);  // all allocation happens in create
+    if (prev >= 0) cudaSetDevice(prev);
+    if (st) {
+        fft3d_b200_plan_destroy(p);
+        set_status(st);
+        return nullptr;
+    }
+    fft3d_plan *h = new fft3d_plan{p};
+    return h;
+}
+
+extern "C" void fft3d_execute(fft3d_plan *plan, const FFT3D_COMPLEX *in, FFT3D_COMPLEX *out)
+{
+    if (!plan) {
+        set_status(FFT3D_B200_ERR_INVALID);
+        return;
+    }
+    const int st = fft3d_b200_execute_host(plan->p, in, out);
+    if (st != FFT3D_B200_OK)
+        fprintf(stderr, "fft3d_execute: %s\n", fft3d_b200_status_string(st));
+}
+
+extern "C" void fft3d_destroy(fft3d_plan *plan)
+{
+    if (!plan) return;
+    fft3d_b200_plan_destroy(plan->p);
+    delete plan;
+}
+
+// ------------------------------------------------------------------ reference contract, device pointers
+
+struct fft3d_gpu_plan {
+    fft3d_b200_plan *p;
+};
+
+extern "C" const char *fft3d_gpu_name(void) { return kName; }
+extern "C" const char *fft3d_gpu_description(void) { return kDesc; }
+extern "C" int fft3d_gpu_supports(int L) { return fft3d_b200_supports(L, L, L, FFT3D_B200_C128); }
+
+extern "C" fft3d_gpu_plan *fft3d_gpu_create(int L, int batch)
+{
+    if (L < 1 || batch < 1) {
+        set_status(FFT3D_B200_ERR_INVALID);
+        return nullptr;
+    }
+    fft3d_b200_desc d = {L, L, L, batch, FFT3D_B200_FORWARD, FFT3D_B200_C128, 0u, -1};
+    fft3d_b200_plan *p = nullptr;
+    if (fft3d_b200_plan_create(&d, &p) != FFT3D_B200_OK) return nullptr;
+    return new fft3d_gpu_plan{p};
+}
+
+// Enqueued on the legacy default stream, which orders it after the caller's
+// cudaMemcpy/cudaMemset on that stream, as the reference driver relies on
+// (bench/gpu/driver.cu:230-253).
+extern "C" void fft3d_gpu_execute(fft3d_gpu_plan *plan, const double2 *in, double2 *out)
+{
+    if (!plan) {
+        set_status(FFT3D_B200_ERR_INVALID);
+        return;
+    }
+    fft3d_b200_execute(plan->p, in, out, (void *)cudaStreamLegacy);
+}
+
+extern "C" void fft3d_gpu_destroy(fft3d_gpu_plan *plan)
+{
+    if (!plan) return;
+    fft3d_b200_plan_destroy(plan->p);
+    delete plan;
+}

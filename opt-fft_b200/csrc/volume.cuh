@@ -1,0 +1,135 @@
+// volume.cuh -- shared-memory layout and the three axis passes of one volume.
+//
+// The row-column structure of the reference (python/fft3d.py:349-399: a 1D
+// transform along every line of each axis in turn) applied to volumes resident
+// in one CTA's shared memory.  The functions here are __host__ __device__ so the
+// CPU unit tests exercise exactly the index arithmetic the kernels run.
+//
+// Shared-memory layout of VPC volumes, row r = (vol*N0 + x)*N1 + y holding the
+// N2 points of one z-line.  One pass reads each line with one thread, so the
+// layout must keep the threads of one access phase on distinct bank groups
+// (8 lanes x 16 B for complex double, 16 lanes x 8 B for complex float):
+//   POL 0  N2 odd:                     natural, row pitch N2 (odd strides never collide)
+//   POL 1  N2 even, not a multiple of the phase width: row pitch N2 + 1
+//   POL 2  N2 a multiple of the phase width: pitch N2, point z stored at
+//          z ^ (r mod width) -- an XOR swizzle, no padding
+#pragma once
+
+#include "codelets.cuh"
+
+namespace fft3d {
+
+template <int N0_, int N1_, int N2_, typename T_>
+struct Geom {
+    using T = T_;
+    static constexpr int N0 = N0_, N1 = N1_, N2 = N2_;
+    static constexpr int V = N0 * N1 * N2;
+    static constexpr int ROWS = N0 * N1;
+    static constexpr int EB = 2 * (int)sizeof(T);
+    static constexpr int GROUP = (EB == 16) ? 8 : 16;
+    static constexpr int POL = (N2 % 2 == 1) ? 0 : ((N2 % GROUP == 0) ? 2 : 1);
+    static constexpr int P2 = (POL == 1) ? N2 + 1 : N2;
+    static constexpr int PV = ROWS * P2;  // shared-memory elements per volume
+
+    FFT_HD static int off(int r, int z)
+    {
+        if constexpr (POL == 2) return r * N2 + (z ^ (r & (GROUP - 1)));
+        else return r * P2 + z;
+    }
+};
+
+// Pass along z for row r (lines are rows).
+template <class G, int S, int ALG>
+FFT_HD void pass_z(cx<typename G::T> *sm, int r)
+{
+    using T = typename G::T;
+    cx<T> v[G::N2];
+#pragma unroll
+    for (int j = 0; j < G::N2; ++j) v[j] = sm[G::off(r, j)];
+    dft<G::N2, S, T, ALG>(v);
+#pragma unroll
+    for (int j = 0; j < G::N2; ++j) sm[G::off(r, j)] = v[j];
+}
+
+// Pass along y for line l = (vol*N0 + x)*N2 + z.
+template <class G, int S, int ALG>
+FFT_HD void pass_y(cx<typename G::T> *sm, int l)
+{
+    using T = typename G::T;
+    const int z = l % G::N2;
+    const int rb = (l / G::N2) * G::N1;
+    cx<T> v[G::N1];
+#pragma unroll
+    for (int j = 0; j < G::N1; ++j) v[j] = sm[G::off(rb + j, z)];
+    dft<G::N1, S, T, ALG>(v);
+#pragma unroll
+    for (int j = 0; j < G::N1; ++j) sm[G::off(rb + j, z)] = v[j];
+}
+
+// Pass along x for line l = (vol*N1 + y)*N2 + z, read from shared memory and
+// written straight to the output volume: consecutive l are consecutive (y, z),
+// so each store instruction of a warp covers a contiguous range.
+template <typename T>
+FFT_HD void store_out(cx<T> *p, cx<T> v)
+{
+#if defined(__CUDA_ARCH__)
+    if constexpr (sizeof(T) == 8) {
+        __stcs(reinterpret_cast<double2 *>(p), make_double2(v.re, v.im));
+    } else {
+        __stcs(reinterpret_cast<float2 *>(p), make_float2(v.re, v.im));
+    }
+#else
+    *p = v;
+#endif
+}
+
+template <typename T>
+FFT_HD cx<T> load_in(const cx<T> *p)
+{
+#if defined(__CUDA_ARCH__)
+    if constexpr (sizeof(T) == 8) {
+        const double2 t = __ldcs(reinterpret_cast<const double2 *>(p));
+        return {t.x, t.y};
+    } else {
+        const float2 t = __ldcs(reinterpret_cast<const float2 *>(p));
+        return {t.x, t.y};
+    }
+#else
+    return *p;
+#endif
+}
+
+template <class G, int S, int ALG>
+FFT_HD void pass_x_out(const cx<typename G::T> *sm, int l, cx<typename G::T> *gout,
+                       typename G::T scale)
+{
+    using T = typename G::T;
+    const int z = l % G::N2;
+    const int t = l / G::N2;
+    const int y = t % G::N1;
+    const int vol = t / G::N1;
+    cx<T> v[G::N0];
+#pragma unroll
+    for (int j = 0; j < G::N0; ++j) v[j] = sm[G::off((vol * G::N0 + j) * G::N1 + y, z)];
+    dft<G::N0, S, T, ALG>(v);
+    cx<T> *o = gout + (long long)vol * G::V + y * G::N2 + z;
+#pragma unroll
+    for (int j = 0; j < G::N0; ++j) {
+        cx<T> r = v[j];
+        if constexpr (S > 0) r = cscale(r, scale);
+        store_out(o + j * (G::N1 * G::N2), r);
+    }
+}
+
+// Copy element g (in [0, nv*V)) of the CTA's input slice into its layout slot.
+template <class G>
+FFT_HD void stage_in(cx<typename G::T> *sm, const cx<typename G::T> *gin, int g)
+{
+    const int vol = g / G::V;
+    const int rem = g - vol * G::V;
+    const int r = vol * G::ROWS + rem / G::N2;
+    const int z = rem % G::N2;
+    sm[G::off(r, z)] = load_in(gin + g);
+}
+
+}  // namespace fft3d

@@ -1,0 +1,92 @@
+// volume_kernels.cu -- kernel family VOLUME: one CTA transforms VPC whole volumes.
+//
+// Per CTA: the CTA's VPC volumes are read from HBM once with coalesced vector
+// loads into the bank-conflict-free shared-memory layout of volume.cuh; the z and
+// y passes run shared memory -> registers -> shared memory, one line per thread;
+// the x pass reads shared memory and writes each result line straight to HBM with
+// coalesced streaming stores, so each volume is written once.  This is the
+// row-column structure of python/fft3d.py:349-399 and of the fused A100 kernels of
+// the reference (bench/gpu/impl_4/L17_dmma.cu:36-38), laid out for sm_100a.
+#include "internal.h"
+#include "volume.cuh"
+
+namespace fft3d {
+
+template <class G, int S, int ALG, int VPC, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
+    k_volume(const cx<typename G::T> *__restrict__ in, cx<typename G::T> *__restrict__ out,
+             long long nvol, typename G::T scale)
+{
+    using T = typename G::T;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);
+
+    const long long v0 = (long long)blockIdx.x * VPC;
+    const long long left = nvol - v0;
+    const int nv = left < VPC ? (int)left : VPC;
+    const cx<T> *gin = in + v0 * G::V;
+    cx<T> *gout = out + v0 * G::V;
+    const int tid = threadIdx.x;
+
+    const int nel = nv * G::V;
+    for (int g = tid; g < nel; g += NT) stage_in<G>(sm, gin, g);
+    __syncthreads();
+    for (int r = tid; r < nv * G::ROWS; r += NT) pass_z<G, S, ALG>(sm, r);
+    __syncthreads();
+    for (int l = tid; l < nv * G::N0 * G::N2; l += NT) pass_y<G, S, ALG>(sm, l);
+    __syncthreads();
+    for (int l = tid; l < nv * G::N1 * G::N2; l += NT) pass_x_out<G, S, ALG>(sm, l, gout, scale);
+}
+
+template <int N0, int N1, int N2, typename T, int S, int ALG, int VPC, int NT, int MINB>
+static void add_volume(std::vector<KernelEntry> &out, const char *name)
+{
+    using G = Geom<N0, N1, N2, T>;
+    KernelEntry e;
+    e.n0 = N0;
+    e.n1 = N1;
+    e.n2 = N2;
+    e.precision = sizeof(T) == 8 ? FFT3D_B200_C128 : FFT3D_B200_C64;
+    e.sign = S;
+    e.family = FAM_VOLUME;
+    e.alg = ALG;
+    e.vpc = VPC;
+    e.threads = NT;
+    e.smem = VPC * G::PV * G::EB;
+    e.func = (const void *)&k_volume<G, S, ALG, VPC, NT, MINB>;
+    e.name = name;
+    out.push_back(e);
+}
+
+// Both directions of one variant.
+#define FFT3D_VOL(N0, N1, N2, T, ALG, VPC, NT, MINB)                                              \
+    add_volume<N0, N1, N2, T, -1, ALG, VPC, NT, MINB>(                                            \
+        out, "volume " #N0 "x" #N1 "x" #N2 " " #T " alg" #ALG " vpc" #VPC " nt" #NT " minb" #MINB); \
+    add_volume<N0, N1, N2, T, +1, ALG, VPC, NT, MINB>(                                            \
+        out, "volume " #N0 "x" #N1 "x" #N2 " " #T " alg" #ALG " vpc" #VPC " nt" #NT " minb" #MINB)
+
+void register_kernels(std::vector<KernelEntry> &out)
+{
+    // complex double
+    FFT3D_VOL(6, 6, 6, double, 0, 16, 256, 1);
+    FFT3D_VOL(8, 8, 8, double, 0, 8, 256, 1);
+    FFT3D_VOL(8, 8, 8, double, 0, 16, 512, 1);
+    FFT3D_VOL(12, 12, 12, double, 0, 2, 288, 1);
+    FFT3D_VOL(16, 16, 16, double, 0, 1, 256, 1);
+    FFT3D_VOL(17, 17, 17, double, 0, 1, 320, 1);
+    FFT3D_VOL(17, 17, 17, double, 1, 1, 320, 1);
+    FFT3D_VOL(24, 24, 24, double, 0, 1, 288, 1);
+    FFT3D_VOL(8, 8, 16, double, 0, 8, 512, 1);
+    FFT3D_VOL(16, 16, 32, double, 0, 1, 256, 1);
+    // complex float
+    FFT3D_VOL(6, 6, 6, float, 0, 32, 512, 1);
+    FFT3D_VOL(8, 8, 8, float, 0, 16, 512, 1);
+    FFT3D_VOL(12, 12, 12, float, 0, 4, 576, 1);
+    FFT3D_VOL(16, 16, 16, float, 0, 2, 512, 1);
+    FFT3D_VOL(17, 17, 17, float, 0, 2, 608, 1);
+    FFT3D_VOL(24, 24, 24, float, 0, 1, 576, 1);
+    FFT3D_VOL(8, 8, 16, float, 0, 16, 1024, 1);
+    FFT3D_VOL(16, 16, 32, float, 0, 1, 512, 1);
+}
+
+}  // namespace fft3d

@@ -1,0 +1,256 @@
+"""Python binding of libfft3d_b200.so, the B200 batched 3D complex FFT.
+
+A thin ctypes layer over the C ABI (include/fft3d_b200.h, fft3d_api.h,
+fft3d_gpu_api.h).  The arithmetic is the CUDA library's; nothing here computes a
+transform.  If the shared library is missing the import fails loudly -- there is
+no CPU fallback.
+
+    import fft3d_b200 as fb
+    plan = fb.Plan((17, 17, 17), batch=2048, direction=fb.FORWARD, precision=fb.C128)
+    plan.execute(d_in_ptr, d_out_ptr, stream_ptr)     # device pointers (ints)
+    out = plan.execute_host(x)                        # numpy in, numpy out
+
+Device buffers are plain integers (e.g. ``torch_tensor.data_ptr()``), so this
+module needs neither torch nor numpy to import.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.environ.get("FFT3D_B200_LIB",
+                          os.path.join(os.path.dirname(_HERE), "libfft3d_b200.so"))
+
+OK = 0
+ERR_INVALID = -1
+ERR_UNSUPPORTED = -2
+ERR_ALIGN = -3
+ERR_CUDA = -4
+ERR_NOMEM = -5
+ERR_TIMEOUT = -6
+ERR_BUDGET = -7
+ERR_OVERLAP = -8
+ERR_BUSY = -9
+
+FORWARD = -1
+BACKWARD = +1
+C128 = 0
+C64 = 1
+FLAG_NO_TUNE = 0x1
+FLAG_NO_GRAPH = 0x2
+
+ELEMENT_BYTES = {C128: 16, C64: 8}
+
+
+class Fft3dError(RuntimeError):
+    def __init__(self, status, what=""):
+        self.status = status
+        msg = _lib.fft3d_b200_status_string(status).decode() if _lib else str(status)
+        super().__init__(f"{what}: {msg} ({status})" if what else f"{msg} ({status})")
+
+
+class Desc(ctypes.Structure):
+    _fields_ = [("n0", ctypes.c_int), ("n1", ctypes.c_int), ("n2", ctypes.c_int),
+                ("batch", ctypes.c_longlong), ("direction", ctypes.c_int),
+                ("precision", ctypes.c_int), ("flags", ctypes.c_uint), ("device", ctypes.c_int)]
+
+
+class Segment(ctypes.Structure):
+    _fields_ = [("n0", ctypes.c_int), ("n1", ctypes.c_int), ("n2", ctypes.c_int),
+                ("direction", ctypes.c_int), ("precision", ctypes.c_int),
+                ("batch", ctypes.c_longlong), ("in_", ctypes.c_void_p), ("out", ctypes.c_void_p)]
+
+
+# Every symbol the headers in include/ declare, by header.
+EXPORTS = {
+    "fft3d_api.h": ["fft3d_name", "fft3d_description", "fft3d_supports", "fft3d_create",
+                    "fft3d_execute", "fft3d_destroy"],
+    "fft3d_gpu_api.h": ["fft3d_gpu_name", "fft3d_gpu_description", "fft3d_gpu_supports",
+                        "fft3d_gpu_create", "fft3d_gpu_execute", "fft3d_gpu_destroy"],
+    "fft3d_b200.h": ["fft3d_b200_supports", "fft3d_b200_plan_create", "fft3d_b200_plan_destroy",
+                     "fft3d_b200_variants", "fft3d_b200_plan_create_variant",
+                     "fft3d_b200_execute", "fft3d_b200_execute_host",
+                     "fft3d_b200_execute_host_chain", "fft3d_b200_plan_describe",
+                     "fft3d_b200_plan_launches", "fft3d_b200_last_status",
+                     "fft3d_b200_status_string", "fft3d_b200_batch_create",
+                     "fft3d_b200_batch_execute", "fft3d_b200_batch_destroy",
+                     "fft3d_b200_batch_describe"],
+}
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python opt-fft_b200/build.py` "
+                          "(there is no CPU fallback)")
+    lib = ctypes.CDLL(LIB_PATH)
+    vp, i, ll = ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong
+    sig = {
+        "fft3d_name": ([], ctypes.c_char_p),
+        "fft3d_description": ([], ctypes.c_char_p),
+        "fft3d_supports": ([i], i),
+        "fft3d_create": ([i, i], vp),
+        "fft3d_execute": ([vp, vp, vp], None),
+        "fft3d_destroy": ([vp], None),
+        "fft3d_gpu_name": ([], ctypes.c_char_p),
+        "fft3d_gpu_description": ([], ctypes.c_char_p),
+        "fft3d_gpu_supports": ([i], i),
+        "fft3d_gpu_create": ([i, i], vp),
+        "fft3d_gpu_execute": ([vp, vp, vp], None),
+        "fft3d_gpu_destroy": ([vp], None),
+        "fft3d_b200_supports": ([i, i, i, i], i),
+        "fft3d_b200_plan_create": ([ctypes.POINTER(Desc), ctypes.POINTER(vp)], i),
+        "fft3d_b200_plan_destroy": ([vp], None),
+        "fft3d_b200_variants": ([i, i, i, i, i, ctypes.POINTER(ctypes.c_char_p), i], i),
+        "fft3d_b200_plan_create_variant": ([ctypes.POINTER(Desc), ctypes.c_char_p,
+                                            ctypes.POINTER(vp)], i),
+        "fft3d_b200_execute": ([vp, vp, vp, vp], i),
+        "fft3d_b200_execute_host": ([vp, vp, vp], i),
+        "fft3d_b200_execute_host_chain": ([ctypes.POINTER(vp), i, vp, vp], i),
+        "fft3d_b200_plan_describe": ([vp], ctypes.c_char_p),
+        "fft3d_b200_plan_launches": ([vp], i),
+        "fft3d_b200_last_status": ([], i),
+        "fft3d_b200_status_string": ([i], ctypes.c_char_p),
+        "fft3d_b200_batch_create": ([ctypes.POINTER(Segment), i, ctypes.c_uint, i,
+                                     ctypes.POINTER(vp)], i),
+        "fft3d_b200_batch_execute": ([vp, vp], i),
+        "fft3d_b200_batch_destroy": ([vp], None),
+        "fft3d_b200_batch_describe": ([vp], ctypes.c_char_p),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    _ = ll
+    return lib
+
+
+_lib = _load()
+
+
+def lib():
+    """The loaded ctypes library."""
+    return _lib
+
+
+def supports(shape, precision=C128) -> bool:
+    n0, n1, n2 = shape
+    return bool(_lib.fft3d_b200_supports(n0, n1, n2, precision))
+
+
+def variants(shape, precision=C128, direction=FORWARD):
+    """Names of the compiled kernel variants the autotuner chooses among."""
+    n0, n1, n2 = shape
+    n = _lib.fft3d_b200_variants(n0, n1, n2, precision, direction, None, 0)
+    arr = (ctypes.c_char_p * max(n, 1))()
+    _lib.fft3d_b200_variants(n0, n1, n2, precision, direction, arr, n)
+    return [arr[k].decode() for k in range(n)]
+
+
+def _check(status, what):
+    if status != OK:
+        raise Fft3dError(status, what)
+
+
+class Plan:
+    """A plan for `batch` volumes of `shape` = (n0, n1, n2)."""
+
+    def __init__(self, shape, batch, direction=FORWARD, precision=C128, flags=0, device=-1,
+                 variant=None):
+        n0, n1, n2 = (int(s) for s in shape)
+        self.shape = (n0, n1, n2)
+        self.batch = int(batch)
+        self.direction = direction
+        self.precision = precision
+        self.elem_bytes = ELEMENT_BYTES.get(precision, 16)
+        self.nbytes = self.batch * n0 * n1 * n2 * self.elem_bytes
+        d = Desc(n0, n1, n2, self.batch, direction, precision, flags, device)
+        h = ctypes.c_void_p()
+        if variant is None:
+            _check(_lib.fft3d_b200_plan_create(ctypes.byref(d), ctypes.byref(h)), "plan_create")
+        else:
+            _check(_lib.fft3d_b200_plan_create_variant(ctypes.byref(d), variant.encode(),
+                                                       ctypes.byref(h)), "plan_create_variant")
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def describe(self) -> str:
+        return _lib.fft3d_b200_plan_describe(self._h).decode()
+
+    def launches(self) -> int:
+        return _lib.fft3d_b200_plan_launches(self._h)
+
+    def execute(self, d_in: int, d_out: int, stream: int = 0):
+        """Enqueue on `stream` (a cudaStream_t as int; 0 = legacy default stream)."""
+        _check(_lib.fft3d_b200_execute(self._h, d_in, d_out, stream or None), "execute")
+
+    def execute_host(self, x, out=None):
+        """numpy in (complex128 for C128, complex64 for C64), numpy out."""
+        import numpy as np
+        dt = np.complex128 if self.precision == C128 else np.complex64
+        x = np.ascontiguousarray(x, dtype=dt)
+        if x.nbytes != self.nbytes:
+            raise ValueError(f"expected {self.nbytes} bytes, got {x.nbytes}")
+        if out is None:
+            out = np.empty_like(x)
+        _check(_lib.fft3d_b200_execute_host(self._h, x.ctypes.data, out.ctypes.data),
+               "execute_host")
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.fft3d_b200_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def execute_host_chain(plans, x, out=None):
+    """Upload x once, run plans back to back on the device, download once."""
+    import numpy as np
+    x = np.ascontiguousarray(x)
+    if out is None:
+        out = np.empty_like(x)
+    arr = (ctypes.c_void_p * len(plans))(*[p.handle.value for p in plans])
+    _check(_lib.fft3d_b200_execute_host_chain(arr, len(plans), x.ctypes.data, out.ctypes.data),
+           "execute_host_chain")
+    return out
+
+
+class Batch:
+    """One persistent launch over segments of uneven geometry (device pointers)."""
+
+    def __init__(self, segments, flags=0, device=-1):
+        arr = (Segment * len(segments))()
+        for k, s in enumerate(segments):
+            arr[k] = Segment(s["shape"][0], s["shape"][1], s["shape"][2],
+                             s.get("direction", FORWARD), s.get("precision", C128),
+                             int(s["batch"]), s["in"], s["out"])
+        h = ctypes.c_void_p()
+        _check(_lib.fft3d_b200_batch_create(arr, len(segments), flags, device, ctypes.byref(h)),
+               "batch_create")
+        self._h = h
+
+    def execute(self, stream: int = 0):
+        _check(_lib.fft3d_b200_batch_execute(self._h, stream or None), "batch_execute")
+
+    def describe(self) -> str:
+        return _lib.fft3d_b200_batch_describe(self._h).decode()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.fft3d_b200_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

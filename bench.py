@@ -108,7 +108,7 @@ class ClockSampler:
             os.close(fd)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200", "-f", self.path],
+                 "--format=csv,noheader,nounits", "-lms", "50", "-f", self.path],
                 stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -151,12 +151,18 @@ class ClockSampler:
 class Workload:
     """Plans and device buffers for one workload on this rank's GPU."""
 
-    def __init__(self, fb, torch, name, device, seed):
+    def __init__(self, fb, torch, name, device, seed, variant=None):
         w = WORKLOADS[name]
         self.name, self.w = name, w
         self.torch, self.fb = torch, fb
         self.shape, self.batch, self.prec = w["shape"], w["batch"], w["prec"]
-        self.plans = [fb.Plan(self.shape, self.batch, d, self.prec) for d in w["chain"]]
+        self.plans = []
+        for d in w["chain"]:
+            v = None
+            if variant:
+                # the same variant name exists for both directions
+                v = variant if variant in fb.variants(self.shape, self.prec, d) else None
+            self.plans.append(fb.Plan(self.shape, self.batch, d, self.prec, variant=v))
         ndt = np.complex128 if self.prec == 0 else np.complex64
         tdt = torch.complex128 if self.prec == 0 else torch.complex64
         self.eb = 16 if self.prec == 0 else 8
@@ -314,12 +320,16 @@ def cpu_reference(name, seconds=10.0, threads=None, max_sample=None):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="roundtrip17", choices=sorted(WORKLOADS))
     ap.add_argument("--no-extra", action="store_true", help="skip the per-L workloads")
-    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0,
+                    help="CPU baseline sample length; 0 skips it")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-pointer measurement")
+    ap.add_argument("--variant", default=None,
+                    help="force this kernel variant for the headline plans (profiling)")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
 
@@ -370,7 +380,7 @@ def main():
     peak, peak_kind = peaks()
     traffic = ncu_traffic()
 
-    wl = Workload(fb, torch, a.workload, device, seed=1234 + rank)
+    wl = Workload(fb, torch, a.workload, device, seed=1234 + rank, variant=a.variant)
     sampler = ClockSampler(local)
     ms, first_ms, clocks = time_device(torch, wl, stream, a.steps, a.warmup, dist, sampler)
     value = world * wl.batch / (ms * 1e-3)
@@ -383,10 +393,12 @@ def main():
                 "traffic": traffic.get(a.workload.replace("roundtrip", "fwd")),
                 "ms_per_launch": first_ms}
 
-    e2e_s, h2d, d2h = time_e2e(fb, torch, wl, max(3, a.steps // 2), 2, dist)
-    e2e = {"value": world * wl.batch / e2e_s, "unit": "volumes/s", "h2d_bytes_per_step": h2d,
-           "d2h_bytes_per_step": d2h,
-           "path": "fft3d_b200_execute_host_chain, page-locked host buffers"}
+    e2e = None
+    if not a.no_e2e:
+        e2e_s, h2d, d2h = time_e2e(fb, torch, wl, max(3, min(50, a.steps // 4)), 2, dist)
+        e2e = {"value": world * wl.batch / e2e_s, "unit": "volumes/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h,
+               "path": "fft3d_b200_execute_host_chain, page-locked host buffers"}
 
     workloads = {}
     if not a.no_extra:
@@ -407,7 +419,7 @@ def main():
             torch.cuda.empty_cache()
 
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and a.cpu_seconds > 0:
         v, kind, thr, desc, _ = cpu_reference(a.workload, seconds=a.cpu_seconds)
         cpu = {"value": v, "unit": "volumes/s", "cores": thr, "kind": kind, "sample": desc}
 

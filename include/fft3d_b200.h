@@ -95,6 +95,10 @@ int fft3d_b200_variants(int n0, int n1, int n2, int precision, int direction, co
 int fft3d_b200_plan_create_variant(const fft3d_b200_desc *desc, const char *variant,
                                    fft3d_b200_plan **out);
 
+/* Wait for the plan's device work and report a device-side failure recorded
+ * since the last check (FFT3D_B200_ERR_TIMEOUT when a bounded wait ran out). */
+int fft3d_b200_plan_check(fft3d_b200_plan *plan);
+
 /* Human-readable description of the kernel configuration the plan selected. */
 const char *fft3d_b200_plan_describe(const fft3d_b200_plan *plan);
 

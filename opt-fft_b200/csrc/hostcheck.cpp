@@ -39,7 +39,51 @@ static void emulate(const void *vin, void *vout, long long nvol)
     }
 }
 
+// The CLUSTER kernel's data movement: C slabs of PL = N0/C planes, local z and y
+// passes, x lines split n1*n2/C per rank and gathered from the owning slabs.
+template <int N0, int N1, int N2, typename T, int S, int C>
+static void emulate_cluster(const void *vin, void *vout, long long nvol)
+{
+    constexpr int PL = N0 / C;
+    using SG = Geom<PL, N1, N2, T>;
+    constexpr int V = N0 * N1 * N2;
+    constexpr int LPC = N1 * N2 / C;
+    const cx<T> *in = (const cx<T> *)vin;
+    cx<T> *out = (cx<T> *)vout;
+    const T scale = S > 0 ? T(1) / T(V) : T(1);
+    std::vector<std::vector<cx<T>>> slab(C, std::vector<cx<T>>(SG::PV));
+    for (long long vol = 0; vol < nvol; ++vol) {
+        for (int rank = 0; rank < C; ++rank) {
+            cx<T> *sm = slab[rank].data();
+            for (auto &e : slab[rank]) e = {T(12345.0), T(-6789.0)};
+            const cx<T> *gin = in + vol * V + (long long)rank * PL * N1 * N2;
+            for (int g = 0; g < PL * N1 * N2; ++g) sm[SG::off(g / N2, g % N2)] = gin[g];
+            for (int r = 0; r < PL * N1; ++r) pass_z<SG, S, ALG_DEFAULT>(sm, r);
+            for (int l = 0; l < PL * N2; ++l) pass_y<SG, S, ALG_DEFAULT>(sm, l);
+        }
+        cx<T> *gout = out + vol * V;
+        for (int rank = 0; rank < C; ++rank) {
+            for (int l = rank * LPC; l < (rank + 1) * LPC; ++l) {
+                const int y = l / N2, z = l % N2;
+                cx<T> v[N0];
+                for (int j = 0; j < N0; ++j) v[j] = slab[j / PL][SG::off((j % PL) * N1 + y, z)];
+                dft<N0, S, T>(v);
+                for (int j = 0; j < N0; ++j) {
+                    cx<T> r = v[j];
+                    if (S > 0) r = cscale(r, scale);
+                    gout[(long long)(j * N1 + y) * N2 + z] = r;
+                }
+            }
+        }
+    }
+}
+
 typedef void (*emu_fn)(const void *, void *, long long);
+
+#define EMU_CL(N0, N1, N2, T, C)                                                             \
+    {N0, N1, N2, sizeof(T) == 8 ? 0 : 1, -1, 100 + C, 1,                                   \
+     &emulate_cluster<N0, N1, N2, T, -1, C>},                                               \
+    {N0, N1, N2, sizeof(T) == 8 ? 0 : 1, +1, 100 + C, 1, &emulate_cluster<N0, N1, N2, T, +1, C>}
 
 struct EmuEntry {
     int n0, n1, n2, prec, sign, alg, vpc;
@@ -62,6 +106,8 @@ static const EmuEntry kEmu[] = {
     EMU(32, 8, 4, double, 0, 1),   EMU(13, 5, 8, double, 0, 1),    EMU(4, 4, 4, double, 0, 2),
     EMU(1, 8, 8, double, 0, 1),    EMU(8, 1, 8, double, 0, 1),     EMU(8, 8, 1, double, 0, 1),
     EMU(1, 1, 1, double, 0, 1),    EMU(3, 3, 3, double, 0, 1),     EMU(17, 2, 2, double, 0, 1),
+    EMU_CL(36, 36, 36, double, 4), EMU_CL(36, 36, 36, double, 6),  EMU_CL(36, 36, 36, double, 9),
+    EMU_CL(36, 36, 36, float, 2),  EMU_CL(36, 36, 36, float, 4),   EMU_CL(36, 36, 36, float, 6),
 };
 
 extern "C" int hostcheck_fft3d(int n0, int n1, int n2, int prec, int sign, int alg, int vpc,

@@ -20,6 +20,7 @@ int ensure_device_tables(int device);
 enum Family : int {
     FAM_VOLUME = 0,   // one CTA transforms VPC whole volumes held in its shared memory
     FAM_CLUSTER = 1,  // a thread-block cluster shares one volume through distributed smem
+    FAM_STREAM = 2,   // persistent CTAs, two-stage pipeline: load of the next group in flight
 };
 
 // One compiled kernel variant.  The plan's autotuner times the entries that
@@ -40,11 +41,16 @@ struct KernelEntry {
 // Registry of every compiled variant (defined by the kernel translation units).
 const std::vector<KernelEntry> &registry();
 void register_kernels(std::vector<KernelEntry> &out);          // volume_kernels.cu
+void register_stream_kernels(std::vector<KernelEntry> &out);   // stream_kernels.cu
 void register_cluster_kernels(std::vector<KernelEntry> &out);  // cluster_kernels.cu
 
 // Launch `e` over `nvol` volumes.  scale multiplies every output (1/V for inverse).
+// Persistent families use at most `grid_limit` CTAs; `err` is the device error word.
 cudaError_t launch_entry(const KernelEntry &e, const void *in, void *out, long long nvol,
-                         double scale, cudaStream_t stream, int num_sms);
+                         double scale, cudaStream_t stream, int grid_limit, int *err);
+
+// CTAs of `e` that fit on one SM (0 if it cannot launch); sets attributes on first use.
+int entry_occupancy(const KernelEntry &e, int device);
 
 int element_bytes(int precision);
 

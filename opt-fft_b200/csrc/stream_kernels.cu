@@ -1,0 +1,231 @@
+// stream_kernels.cu -- kernel family STREAM: persistent CTAs with an NSTAGE-deep
+// shared-memory ring.
+//
+// Each CTA walks the volume groups (VPC volumes each) item = blockIdx.x +
+// k*gridDim.x.  While the three passes of item k run out of stage k % NSTAGE, the
+// loads of items k+1 .. k+NSTAGE-1 are already in flight into the other stages,
+// so HBM reads overlap the arithmetic; the x pass writes results straight to HBM
+// with coalesced streaming stores, so a stage is free again as soon as its last
+// pass has read it.  NSTAGE = 1 with MINB = 2 puts two single-stage CTAs on an
+// SM instead: one loads while the other computes.
+//
+// Loaders:
+//   BULK   (natural layout, odd n2): thread 0 issues one cp.async.bulk (TMA)
+//          per item -- the group is one contiguous byte range -- completing on
+//          the stage's mbarrier.  Items that are not 16-byte aligned in address
+//          or size (complex64 tails of odd volumes) are copied by the threads.
+//   ASYNC  (padded or XOR-swizzled layouts): every thread issues cp.async copies
+//          of its elements straight into their layout slots.
+// Every mbarrier wait is bounded (ptx.cuh); a timeout records an error code in
+// the plan's device error word and the CTA leaves after a bounded drain.
+#include "internal.h"
+#include "ptx.cuh"
+#include "volume.cuh"
+
+namespace fft3d {
+
+constexpr int LOADER_BULK = 0;
+constexpr int LOADER_ASYNC = 1;
+
+template <class G, int VPC, int NSTAGE>
+struct StreamLayout {
+    // stage size rounded to 128 bytes; NSTAGE mbarriers after the stages
+    static constexpr int STAGE_BYTES = ((VPC * G::PV * G::EB) + 127) / 128 * 128;
+    static constexpr int SMEM_BYTES = NSTAGE * STAGE_BYTES + 8 * NSTAGE;
+};
+
+// Threads copy element by element (synchronous), used for unaligned BULK items.
+template <class G>
+__device__ __forceinline__ void load_lsu(cx<typename G::T> *stage, const cx<typename G::T> *gin,
+                                         int nel, int tid, int nt)
+{
+    for (int g = tid; g < nel; g += nt) stage_in<G>(stage, gin, g);
+}
+
+template <class G, int NT>
+__device__ __forceinline__ void load_async(cx<typename G::T> *stage, const cx<typename G::T> *gin,
+                                           int nel, int tid)
+{
+    for (int g = tid; g < nel; g += NT) {
+        const int vol = g / G::V;
+        const int rem = g - vol * G::V;
+        const int r = vol * G::ROWS + rem / G::N2;
+        const int z = rem % G::N2;
+        if constexpr (G::EB == 16) cp_async_16(stage + G::off(r, z), gin + g);
+        else cp_async_8(stage + G::off(r, z), gin + g);
+    }
+}
+
+// Wait until at most `pending` cp.async groups of this thread are in flight.
+__device__ __forceinline__ void cp_async_wait_pending(int pending)
+{
+    switch (pending) {
+    case 0: cp_async_wait<0>(); break;
+    case 1: cp_async_wait<1>(); break;
+    case 2: cp_async_wait<2>(); break;
+    default: cp_async_wait<3>(); break;
+    }
+}
+
+template <class G, int S, int ALG, int VPC, int NT, int LOADER, int NSTAGE, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
+    k_stream(const cx<typename G::T> *__restrict__ in, cx<typename G::T> *__restrict__ out,
+             long long nvol, typename G::T scale, int *err)
+{
+    static_assert(NSTAGE >= 1 && NSTAGE <= 4, "ring depth");
+    using T = typename G::T;
+    using SL = StreamLayout<G, VPC, NSTAGE>;
+    extern __shared__ __align__(128) unsigned char smraw[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + NSTAGE * SL::STAGE_BYTES);
+    __shared__ int s_abort;
+    auto stage = [&](int s) { return reinterpret_cast<cx<T> *>(smraw + s * SL::STAGE_BYTES); };
+
+    const int tid = threadIdx.x;
+    const long long nitems = (nvol + VPC - 1) / VPC;
+    const long long stride = gridDim.x;
+    if (tid == 0) {
+        if constexpr (LOADER == LOADER_BULK) {
+            for (int s = 0; s < NSTAGE; ++s) mbar_init(&bar[s], 1);
+            fence_mbar_init();
+        }
+        s_abort = 0;
+    }
+    __syncthreads();
+
+    // Issue the load of `item` into stage s.  For BULK, returns with the copy in
+    // flight (or, for an unaligned item, done by the threads and arrived).
+    auto issue = [&](long long item, int s) {
+        const long long v0 = item * VPC;
+        const int nv = (int)((nvol - v0) < VPC ? (nvol - v0) : VPC);
+        const cx<T> *gin = in + v0 * G::V;
+        const int nel = nv * G::V;
+        if constexpr (LOADER == LOADER_BULK) {
+            const uint32_t bytes = (uint32_t)nel * (uint32_t)G::EB;
+            const bool aligned = ((((uintptr_t)gin) | bytes) & 15u) == 0;
+            if (aligned) {
+                if (tid == 0) {
+                    mbar_arrive_expect_tx(&bar[s], bytes);
+                    bulk_g2s(stage(s), gin, bytes, &bar[s]);
+                }
+            } else {
+                load_lsu<G>(stage(s), gin, nel, tid, NT);
+                __syncthreads();
+                if (tid == 0) mbar_arrive(&bar[s]);
+            }
+        } else {
+            load_async<G, NT>(stage(s), gin, nel, tid);
+            cp_async_commit();
+        }
+    };
+
+    long long item = blockIdx.x;
+    for (int j = 0; j < NSTAGE - 1; ++j)
+        if (item + j * stride < nitems) issue(item + j * stride, j);
+    int k = 0;
+    for (; item < nitems; item += stride, ++k) {
+        const int cur = k % NSTAGE;
+        const long long ahead = item + (long long)(NSTAGE - 1) * stride;
+        if (ahead < nitems) issue(ahead, (k + NSTAGE - 1) % NSTAGE);
+
+        if constexpr (LOADER == LOADER_BULK) {
+            if (!mbar_wait_bounded(&bar[cur], (uint32_t)((k / NSTAGE) & 1))) s_abort = 1;
+        } else {
+            int later = 0;  // groups committed after this item's
+            for (int j = 1; j < NSTAGE; ++j)
+                if (item + j * stride < nitems) ++later;
+            cp_async_wait_pending(later);
+        }
+        __syncthreads();
+        if (s_abort) break;
+
+        const long long v0 = item * VPC;
+        const int nv = (int)((nvol - v0) < VPC ? (nvol - v0) : VPC);
+        cx<T> *sm = stage(cur);
+        for (int r = tid; r < nv * G::ROWS; r += NT) pass_z<G, S, ALG>(sm, r);
+        __syncthreads();
+        for (int l = tid; l < nv * G::N0 * G::N2; l += NT) pass_y<G, S, ALG>(sm, l);
+        __syncthreads();
+        cx<T> *gout = out + v0 * G::V;
+        for (int l = tid; l < nv * G::N1 * G::N2; l += NT) pass_x_out<G, S, ALG>(sm, l, gout, scale);
+        if constexpr (LOADER == LOADER_BULK) fence_proxy_async_smem();
+        __syncthreads();
+    }
+
+    if (s_abort) {
+        if (tid == 0) report_error(err, DEV_ERR_LOAD_TIMEOUT);
+        // bounded drain of the stage that timed out and of the loads issued ahead of it
+        if constexpr (LOADER == LOADER_BULK) {
+            for (int j = 0; j < NSTAGE; ++j)
+                if (item + j * stride < nitems)
+                    mbar_wait_bounded(&bar[(k + j) % NSTAGE], (uint32_t)(((k + j) / NSTAGE) & 1));
+        } else {
+            cp_async_wait<0>();
+        }
+    }
+}
+
+template <int N0, int N1, int N2, typename T, int S, int ALG, int VPC, int NT, int NSTAGE,
+          int MINB>
+static void add_stream(std::vector<KernelEntry> &out, const char *name)
+{
+    using G = Geom<N0, N1, N2, T>;
+    constexpr int LOADER = (G::POL == 0) ? LOADER_BULK : LOADER_ASYNC;
+    KernelEntry e;
+    e.n0 = N0;
+    e.n1 = N1;
+    e.n2 = N2;
+    e.precision = sizeof(T) == 8 ? FFT3D_B200_C128 : FFT3D_B200_C64;
+    e.sign = S;
+    e.family = FAM_STREAM;
+    e.alg = ALG;
+    e.vpc = VPC;
+    e.threads = NT;
+    e.smem = StreamLayout<G, VPC, NSTAGE>::SMEM_BYTES;
+    e.func = (const void *)&k_stream<G, S, ALG, VPC, NT, LOADER, NSTAGE, MINB>;
+    e.name = name;
+    out.push_back(e);
+}
+
+#define FFT3D_STREAM(N0, N1, N2, T, ALG, VPC, NT, NST, MINB)                                      \
+    add_stream<N0, N1, N2, T, -1, ALG, VPC, NT, NST, MINB>(                                       \
+        out, "stream " #N0 "x" #N1 "x" #N2 " " #T " alg" #ALG " vpc" #VPC " nt" #NT " st" #NST   \
+             " minb" #MINB);                                                                      \
+    add_stream<N0, N1, N2, T, +1, ALG, VPC, NT, NST, MINB>(                                       \
+        out, "stream " #N0 "x" #N1 "x" #N2 " " #T " alg" #ALG " vpc" #VPC " nt" #NT " st" #NST   \
+             " minb" #MINB)
+
+void register_stream_kernels(std::vector<KernelEntry> &out)
+{
+    // complex double (ring must fit 227 KB per CTA, MINB CTAs per SM)
+    FFT3D_STREAM(6, 6, 6, double, 0, 8, 288, 3, 1);
+    FFT3D_STREAM(6, 6, 6, double, 0, 16, 576, 2, 1);
+    FFT3D_STREAM(8, 8, 8, double, 0, 4, 256, 4, 1);
+    FFT3D_STREAM(8, 8, 8, double, 0, 2, 128, 3, 2);
+    FFT3D_STREAM(8, 8, 8, double, 0, 8, 512, 2, 1);
+    FFT3D_STREAM(12, 12, 12, double, 0, 2, 288, 2, 1);
+    FFT3D_STREAM(12, 12, 12, double, 0, 1, 160, 3, 2);
+    FFT3D_STREAM(16, 16, 16, double, 0, 1, 256, 2, 1);
+    FFT3D_STREAM(16, 16, 16, double, 0, 1, 256, 3, 1);
+    FFT3D_STREAM(17, 17, 17, double, 0, 1, 320, 2, 1);
+    FFT3D_STREAM(17, 17, 17, double, 1, 1, 320, 2, 1);
+    FFT3D_STREAM(17, 17, 17, double, 0, 1, 320, 1, 2);
+    FFT3D_STREAM(8, 8, 16, double, 0, 4, 512, 2, 1);
+    FFT3D_STREAM(8, 8, 16, double, 0, 2, 256, 4, 1);
+    // complex float
+    FFT3D_STREAM(6, 6, 6, float, 0, 16, 576, 3, 1);
+    FFT3D_STREAM(6, 6, 6, float, 0, 32, 1024, 2, 1);
+    FFT3D_STREAM(8, 8, 8, float, 0, 8, 512, 4, 1);
+    FFT3D_STREAM(8, 8, 8, float, 0, 16, 1024, 2, 1);
+    FFT3D_STREAM(12, 12, 12, float, 0, 2, 288, 4, 1);
+    FFT3D_STREAM(12, 12, 12, float, 0, 4, 576, 2, 1);
+    FFT3D_STREAM(16, 16, 16, float, 0, 1, 256, 4, 1);
+    FFT3D_STREAM(16, 16, 16, float, 0, 2, 512, 2, 1);
+    FFT3D_STREAM(17, 17, 17, float, 0, 2, 640, 2, 1);
+    FFT3D_STREAM(17, 17, 17, float, 1, 2, 640, 2, 1);
+    FFT3D_STREAM(8, 8, 16, float, 0, 4, 512, 4, 1);
+    FFT3D_STREAM(8, 8, 16, float, 0, 8, 512, 2, 1);
+    FFT3D_STREAM(16, 16, 32, float, 0, 1, 256, 2, 1);
+    FFT3D_STREAM(16, 16, 32, float, 0, 1, 256, 3, 1);
+}
+
+}  // namespace fft3d

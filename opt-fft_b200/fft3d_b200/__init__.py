@@ -72,6 +72,7 @@ EXPORTS = {
                      "fft3d_b200_variants", "fft3d_b200_plan_create_variant",
                      "fft3d_b200_execute", "fft3d_b200_execute_host",
                      "fft3d_b200_execute_host_chain", "fft3d_b200_plan_describe",
+                     "fft3d_b200_plan_check",
                      "fft3d_b200_plan_launches", "fft3d_b200_last_status",
                      "fft3d_b200_status_string", "fft3d_b200_batch_create",
                      "fft3d_b200_batch_execute", "fft3d_b200_batch_destroy",
@@ -108,6 +109,7 @@ def _load():
         "fft3d_b200_execute_host": ([vp, vp, vp], i),
         "fft3d_b200_execute_host_chain": ([ctypes.POINTER(vp), i, vp, vp], i),
         "fft3d_b200_plan_describe": ([vp], ctypes.c_char_p),
+        "fft3d_b200_plan_check": ([vp], i),
         "fft3d_b200_plan_launches": ([vp], i),
         "fft3d_b200_last_status": ([], i),
         "fft3d_b200_status_string": ([i], ctypes.c_char_p),
@@ -179,6 +181,10 @@ class Plan:
 
     def describe(self) -> str:
         return _lib.fft3d_b200_plan_describe(self._h).decode()
+
+    def check(self):
+        """Synchronise and raise if a bounded device-side wait ran out."""
+        _check(_lib.fft3d_b200_plan_check(self._h), "plan_check")
 
     def launches(self) -> int:
         return _lib.fft3d_b200_plan_launches(self._h)

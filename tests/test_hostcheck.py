@@ -67,6 +67,21 @@ def test_c64_pass_code(hostcheck, shape, alg, vpc, sign):
     assert err < C64_TOL, err
 
 
+@pytest.mark.parametrize("prec,c", [(0, 4), (0, 6), (0, 9), (1, 2), (1, 4), (1, 6)])
+@pytest.mark.parametrize("sign", [-1, +1])
+def test_cluster_data_movement(hostcheck, prec, c, sign):
+    """The CLUSTER kernel's slab split and distributed x-pass gather (alg = 100 + C)."""
+    shape = (36, 36, 36)
+    rng = np.random.default_rng(3000 + c + prec)
+    dt = np.complex128 if prec == 0 else np.complex64
+    x = field(rng, (2,) + shape, dist="normal", dtype=dt)
+    got = run(hostcheck, x, shape, prec, sign, 100 + c, 1)
+    x64 = x.astype(np.complex128)
+    want = oracle.fft3d(x64) if sign < 0 else oracle.ifft3d(x64)
+    err = oracle.rel_error_per_volume(got, want).max()
+    assert err < (C128_TOL if prec == 0 else C64_TOL), err
+
+
 GOLD = [p for p in sorted(glob.glob(os.path.join(GOLDEN, "vol_*.npz")))]
 
 

@@ -1,29 +1,265 @@
-// batch.cu -- descriptor-list batches of uneven geometry (persistent launch).
+// batch.cu -- descriptor-list batches of uneven geometry: host side.
+//
+// fft3d_b200_batch_create validates the caller's segments, maps each to a
+// compiled kind of batch_kernel.cu, cuts it into items, orders the items largest
+// first, uploads the descriptor list, sizes the persistent grid from occupancy,
+// allocates the per-CTA scratch the two-phase 36^3 kinds need, and captures the
+// ticket reset plus the launch in a CUDA graph.  fft3d_b200_batch_execute
+// replays the graph on the caller's stream: one launch for the whole batch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
 #include "../../include/fft3d_b200.h"
+#include "batch_kinds.h"
 #include "internal.h"
+#include "volume.cuh"
+
+namespace fft3d {
+
+struct KindInfo {
+    int id, n0, n1, n2, prec, sign, vpc, solo, big;
+    long long vol_elems;
+    long long stage_bytes;
+};
+
+template <int N0, int N1, int N2, typename T, int VPC, int BIG>
+constexpr long long kind_stage_bytes()
+{
+    if constexpr (BIG > 0) return (long long)Geom<BIG, N1, N2, T>::PV * Geom<BIG, N1, N2, T>::EB;
+    else return (long long)VPC * Geom<N0, N1, N2, T>::PV * Geom<N0, N1, N2, T>::EB;
+}
+
+static const KindInfo kKinds[] = {
+#define FFT3D_BK_INFO(ID, N0, N1, N2, T, S, VPC, SOLO, BIG)                                   \
+    {ID, N0, N1, N2, sizeof(T) == 8 ? FFT3D_B200_C128 : FFT3D_B200_C64, S, VPC, SOLO, BIG, \
+     (long long)N0 * N1 * N2, kind_stage_bytes<N0, N1, N2, T, VPC, BIG>()},
+    FFT3D_BATCH_KINDS(FFT3D_BK_INFO)
+#undef FFT3D_BK_INFO
+};
+
+static const KindInfo *find_kind(int n0, int n1, int n2, int prec, int sign)
+{
+    for (const auto &k : kKinds)
+        if (k.n0 == n0 && k.n1 == n1 && k.n2 == n2 && k.prec == prec && k.sign == sign) return &k;
+    return nullptr;
+}
+
+}  // namespace fft3d
+
+using namespace fft3d;
 
 struct fft3d_b200_batch {
-    int dummy;
+    int device = 0;
+    std::vector<fft3d_b200_segment> segs;
+    BatchItem *d_items = nullptr;
+    BatchSeg *d_segs = nullptr;
+    unsigned int *d_ticket = nullptr;
+    unsigned char *d_solo = nullptr;
+    unsigned char *d_scratch = nullptr;
+    int *d_err = nullptr;
+    long long scratch_per_cta = 0;
+    int nitems = 0;
+    int grid = 0;
+    bool use_graph = false;
+    cudaStream_t cap = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::string describe;
 };
+
+static void batch_free(fft3d_b200_batch *b)
+{
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    if (b->cap) cudaStreamDestroy(b->cap);
+    cudaFree(b->d_items);
+    cudaFree(b->d_segs);
+    cudaFree(b->d_ticket);
+    cudaFree(b->d_solo);
+    cudaFree(b->d_scratch);
+    cudaFree(b->d_err);
+    delete b;
+}
+
+static cudaError_t batch_enqueue(fft3d_b200_batch *b, cudaStream_t s)
+{
+    cudaError_t e = cudaMemsetAsync(b->d_ticket, 0, sizeof(unsigned int), s);
+    if (e != cudaSuccess) return e;
+    if (b->nitems == 0) return cudaSuccess;
+    const BatchItem *items = b->d_items;
+    int nitems = b->nitems;
+    const BatchSeg *segs = b->d_segs;
+    unsigned int *ticket = b->d_ticket;
+    unsigned char *scratch = b->d_scratch;
+    long long spc = b->scratch_per_cta;
+    const unsigned char *solo = b->d_solo;
+    int *err = b->d_err;
+    void *args[] = {(void *)&items, (void *)&nitems, (void *)&segs,   (void *)&ticket,
+                    (void *)&scratch, (void *)&spc,  (void *)&solo, (void *)&err};
+    return cudaLaunchKernel(batch_kernel_func(), dim3(b->grid), dim3(batch_kernel_threads()), args,
+                            (size_t)batch_kernel_smem(), s);
+}
 
 extern "C" int fft3d_b200_batch_create(const fft3d_b200_segment *segs, int nseg, unsigned flags,
                                        int device, fft3d_b200_batch **out)
 {
-    (void)segs; (void)nseg; (void)flags; (void)device;
-    if (out) *out = nullptr;
-    return FFT3D_B200_ERR_UNSUPPORTED;
+    if (!out) return FFT3D_B200_ERR_INVALID;
+    *out = nullptr;
+    if (nseg < 0 || (nseg > 0 && !segs)) return FFT3D_B200_ERR_INVALID;
+    std::vector<BatchItem> items;
+    std::vector<BatchSeg> dsegs;
+    std::vector<unsigned char> solo(BATCH_NKINDS, 0);
+    long long scratch_need = 0;
+    for (int k = 0; k < BATCH_NKINDS; ++k) {
+        const KindInfo &ki = kKinds[k];
+        if (ki.stage_bytes > batch_kernel_smem()) return FFT3D_B200_ERR_UNSUPPORTED;
+        solo[k] = (unsigned char)(ki.solo || ki.big || ki.stage_bytes > batch_kernel_half());
+    }
+    for (int i = 0; i < nseg; ++i) {
+        const fft3d_b200_segment &s = segs[i];
+        if (s.n0 < 1 || s.n1 < 1 || s.n2 < 1 || s.batch < 0) return FFT3D_B200_ERR_INVALID;
+        if (s.direction != FFT3D_B200_FORWARD && s.direction != FFT3D_B200_BACKWARD)
+            return FFT3D_B200_ERR_INVALID;
+        if (s.precision != FFT3D_B200_C128 && s.precision != FFT3D_B200_C64)
+            return FFT3D_B200_ERR_INVALID;
+        const KindInfo *k = find_kind(s.n0, s.n1, s.n2, s.precision, s.direction);
+        if (!k) return FFT3D_B200_ERR_UNSUPPORTED;
+        const size_t eb = (size_t)element_bytes(s.precision);
+        const size_t bytes = (size_t)s.batch * (size_t)k->vol_elems * eb;
+        if (s.batch > 0) {
+            if (!s.in || !s.out) return FFT3D_B200_ERR_INVALID;
+            if (((uintptr_t)s.in % eb) || ((uintptr_t)s.out % eb)) return FFT3D_B200_ERR_ALIGN;
+            const char *a = (const char *)s.in, *o = (const char *)s.out;
+            if (a < o + bytes && o < a + bytes) return FFT3D_B200_ERR_OVERLAP;
+        }
+        BatchSeg d;
+        d.in = s.in;
+        d.out = s.out;
+        d.scale = s.direction == FFT3D_B200_BACKWARD ? 1.0 / (double)k->vol_elems : 1.0;
+        d.nvol = s.batch;
+        d.kind = k->id;
+        d.pad = 0;
+        dsegs.push_back(d);
+        for (long long v0 = 0; v0 < s.batch; v0 += k->vpc) {
+            BatchItem it;
+            it.kind = k->id;
+            it.seg = i;
+            it.v0 = v0;
+            it.nv = (int)std::min<long long>(k->vpc, s.batch - v0);
+            it.pad = 0;
+            items.push_back(it);
+        }
+        if (k->big && s.batch > 0) scratch_need = std::max(scratch_need, (long long)(k->vol_elems * eb));
+    }
+    if (items.size() > 0x7fffffff) return FFT3D_B200_ERR_INVALID;
+    // largest first: big items start early, small ones fill the tail
+    std::stable_sort(items.begin(), items.end(), [](const BatchItem &a, const BatchItem &b) {
+        const KindInfo &ka = kKinds[a.kind], &kb = kKinds[b.kind];
+        const long long ca = (long long)a.nv * ka.vol_elems * (ka.prec == FFT3D_B200_C128 ? 16 : 8);
+        const long long cb = (long long)b.nv * kb.vol_elems * (kb.prec == FFT3D_B200_C128 ? 16 : 8);
+        return ca > cb;
+    });
+
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (device < 0) device = prev < 0 ? 0 : prev;
+    if (cudaSetDevice(device) != cudaSuccess) return FFT3D_B200_ERR_CUDA;
+    int st = ensure_device_tables(device);
+    if (st) {
+        if (prev >= 0) cudaSetDevice(prev);
+        return st;
+    }
+    fft3d_b200_batch *b = new fft3d_b200_batch();
+    b->device = device;
+    b->segs.assign(segs, segs + nseg);
+    b->nitems = (int)items.size();
+    auto fail = [&](int code) {
+        const cudaError_t ce = cudaGetLastError();
+        if (getenv("FFT3D_B200_DEBUG"))
+            fprintf(stderr, "fft3d_b200_batch_create: status %d (%s)\n", code, cudaGetErrorString(ce));
+        batch_free(b);
+        if (prev >= 0) cudaSetDevice(prev);
+        return code;
+    };
+    if (cudaFuncSetAttribute(batch_kernel_func(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             batch_kernel_smem()) != cudaSuccess)
+        return fail(FFT3D_B200_ERR_CUDA);
+    int occ = 0, sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_kernel_func(),
+                                                      batch_kernel_threads(),
+                                                      (size_t)batch_kernel_smem()) != cudaSuccess ||
+        occ < 1)
+        return fail(FFT3D_B200_ERR_UNSUPPORTED);
+    b->grid = std::max(1, std::min(occ * sms, std::max(1, b->nitems)));
+    if (cudaMalloc(&b->d_items, std::max<size_t>(1, items.size()) * sizeof(BatchItem)) != cudaSuccess ||
+        cudaMalloc(&b->d_segs, std::max<size_t>(1, dsegs.size()) * sizeof(BatchSeg)) != cudaSuccess ||
+        cudaMalloc(&b->d_ticket, sizeof(unsigned int)) != cudaSuccess ||
+        cudaMalloc(&b->d_solo, BATCH_NKINDS) != cudaSuccess ||
+        cudaMalloc(&b->d_err, sizeof(int)) != cudaSuccess)
+        return fail(FFT3D_B200_ERR_NOMEM);
+    if (!items.empty() &&
+        cudaMemcpy(b->d_items, items.data(), items.size() * sizeof(BatchItem), cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(FFT3D_B200_ERR_CUDA);
+    if (!dsegs.empty() &&
+        cudaMemcpy(b->d_segs, dsegs.data(), dsegs.size() * sizeof(BatchSeg), cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(FFT3D_B200_ERR_CUDA);
+    if (cudaMemcpy(b->d_solo, solo.data(), BATCH_NKINDS, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(b->d_err, 0, sizeof(int)) != cudaSuccess)
+        return fail(FFT3D_B200_ERR_CUDA);
+    if (scratch_need > 0) {
+        b->scratch_per_cta = (scratch_need + 255) / 256 * 256;
+        if (cudaMalloc(&b->d_scratch, (size_t)b->scratch_per_cta * b->grid) != cudaSuccess)
+            return fail(FFT3D_B200_ERR_NOMEM);
+    }
+    b->use_graph = !(flags & FFT3D_B200_FLAG_NO_GRAPH);
+    if (b->use_graph) {
+        if (cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking) != cudaSuccess)
+            return fail(FFT3D_B200_ERR_CUDA);
+        if (cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+            return fail(FFT3D_B200_ERR_CUDA);
+        cudaError_t le = batch_enqueue(b, b->cap);
+        cudaError_t ee = cudaStreamEndCapture(b->cap, &b->graph);
+        if (le != cudaSuccess || ee != cudaSuccess) return fail(FFT3D_B200_ERR_CUDA);
+        if (cudaGraphInstantiate(&b->exec, b->graph, 0) != cudaSuccess) return fail(FFT3D_B200_ERR_CUDA);
+    }
+    char buf[256];
+    snprintf(buf, sizeof buf, "batch: %d segments, %d items, grid %d x %d threads, %s%s", nseg,
+             b->nitems, b->grid, batch_kernel_threads(), b->use_graph ? "CUDA graph" : "direct launch",
+             b->d_scratch ? ", two-phase scratch" : "");
+    b->describe = buf;
+    if (prev >= 0 && prev != device) cudaSetDevice(prev);
+    *out = b;
+    return FFT3D_B200_OK;
 }
 
 extern "C" int fft3d_b200_batch_execute(fft3d_b200_batch *b, void *stream)
 {
-    (void)b; (void)stream;
-    return FFT3D_B200_ERR_UNSUPPORTED;
+    if (!b) return FFT3D_B200_ERR_INVALID;
+    cudaError_t e;
+    if (b->use_graph) e = cudaGraphLaunch(b->exec, (cudaStream_t)stream);
+    else e = batch_enqueue(b, (cudaStream_t)stream);
+    return e == cudaSuccess ? FFT3D_B200_OK : FFT3D_B200_ERR_CUDA;
 }
 
-extern "C" void fft3d_b200_batch_destroy(fft3d_b200_batch *b) { delete b; }
+extern "C" void fft3d_b200_batch_destroy(fft3d_b200_batch *b)
+{
+    if (!b) return;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(b->device);
+    cudaDeviceSynchronize();
+    batch_free(b);
+    if (prev >= 0) cudaSetDevice(prev);
+}
 
 extern "C" const char *fft3d_b200_batch_describe(const fft3d_b200_batch *b)
 {
-    (void)b;
-    return "";
+    return b ? b->describe.c_str() : "";
 }

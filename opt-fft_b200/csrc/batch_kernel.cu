@@ -1,0 +1,227 @@
+// batch_kernel.cu -- one persistent kernel over a device descriptor list of work
+// items of uneven geometry (extents, precision, direction).
+//
+// The host (batch.cu) cuts every segment into items of VPC volumes of one
+// "kind" (a compiled geometry x precision x direction), sorts the items by
+// bytes, largest first, and uploads them.  Each CTA of the persistent grid takes
+// items with an atomic ticket, so large items start first and small ones fill
+// the tail.  Shared memory is two halves: an item that fits a half is loaded
+// with cp.async while the previous one is transformed out of the other half;
+// larger items (24^3 and 16x16x32 complex double) use all of it.
+//
+// 36^3 does not fit one SM.  In this kernel a single CTA transforms it in two
+// phases through a per-CTA scratch volume in global memory: x-slabs (z and y
+// passes) are written to scratch, then y-slabs are read back for the x pass and
+// written to the output.  The scratch of one CTA stays in L2, so HBM traffic is
+// still about one read and one write of the volume.  (The plain 36^3 path uses
+// the cluster kernel instead, which needs no scratch.)
+#include "internal.h"
+#include "ptx.cuh"
+#include "volume.cuh"
+#include "batch_kinds.h"
+
+namespace fft3d {
+
+constexpr int BATCH_THREADS = 320;
+// 227 KB is the per-CTA maximum on sm_100a, static shared memory included; keep
+// 128 bytes for this kernel's static variables.
+constexpr int BATCH_SMEM = 232448 - 128;
+constexpr int BATCH_HALF = (BATCH_SMEM / 2) / 128 * 128;
+
+// cp.async copy of nel elements into the layout of G (row = g / N2).
+template <class G>
+__device__ __forceinline__ void batch_load(cx<typename G::T> *sm, const cx<typename G::T> *gin,
+                                           int nel)
+{
+    for (int g = threadIdx.x; g < nel; g += BATCH_THREADS) {
+        const int vol = g / G::V;
+        const int rem = g - vol * G::V;
+        cx<typename G::T> *dst = sm + G::off(vol * G::ROWS + rem / G::N2, rem % G::N2);
+        if constexpr (G::EB == 16) cp_async_16(dst, gin + g);
+        else cp_async_8(dst, gin + g);
+    }
+    cp_async_commit();
+}
+
+template <class G, int S>
+__device__ __forceinline__ void batch_passes(cx<typename G::T> *sm, int nv,
+                                             cx<typename G::T> *gout, typename G::T scale)
+{
+    const int tid = threadIdx.x;
+    for (int r = tid; r < nv * G::ROWS; r += BATCH_THREADS) pass_z<G, S, ALG_DEFAULT>(sm, r);
+    __syncthreads();
+    for (int l = tid; l < nv * G::N0 * G::N2; l += BATCH_THREADS) pass_y<G, S, ALG_DEFAULT>(sm, l);
+    __syncthreads();
+    for (int l = tid; l < nv * G::N1 * G::N2; l += BATCH_THREADS)
+        pass_x_out<G, S, ALG_DEFAULT>(sm, l, gout, scale);
+}
+
+// ---------------------------------------------------------------- two-phase large cube
+
+// One L^3 volume by one CTA: NS x-slabs of PL planes, then NS y-slabs of PL rows.
+template <int L, typename T, int S, int PL>
+__device__ __forceinline__ void big_cube(cx<T> *sm, const cx<T> *gin, cx<T> *gout, cx<T> *scratch, T scale)
+{
+    constexpr int NS = L / PL;
+    using XG = Geom<PL, L, L, T>;  // x-slab: PL planes of L x L
+    using YG = Geom<L, PL, L, T>;  // y-slab: all x, PL rows of y
+    const int tid = threadIdx.x;
+    for (int s = 0; s < NS; ++s) {
+        batch_load<XG>(sm, gin + (long long)s * PL * L * L, PL * L * L);
+        cp_async_wait<0>();
+        __syncthreads();
+        for (int r = tid; r < PL * L; r += BATCH_THREADS) pass_z<XG, S, ALG_DEFAULT>(sm, r);
+        __syncthreads();
+        for (int l = tid; l < PL * L; l += BATCH_THREADS) pass_y<XG, S, ALG_DEFAULT>(sm, l);
+        __syncthreads();
+        cx<T> *dst = scratch + (long long)s * PL * L * L;
+        for (int g = tid; g < PL * L * L; g += BATCH_THREADS) dst[g] = sm[XG::off(g / L, g % L)];
+        __syncthreads();
+    }
+    __threadfence();
+    __syncthreads();
+    for (int s = 0; s < NS; ++s) {
+        // rows (x, y - s*PL) of the y-slab; the source rows are L*L apart in scratch
+        for (int g = tid; g < L * PL * L; g += BATCH_THREADS) {
+            const int z = g % L;
+            const int row = g / L;  // x * PL + yl
+            const int x = row / PL, yl = row % PL;
+            cx<T> *d = sm + YG::off(row, z);
+            const cx<T> *src = scratch + ((long long)x * L + s * PL + yl) * L + z;
+            if constexpr (sizeof(T) == 8) cp_async_16(d, src);
+            else cp_async_8(d, src);
+        }
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncthreads();
+        for (int l = tid; l < PL * L; l += BATCH_THREADS) pass_x_slab<YG, S, L>(sm, l, gout, s * PL, scale);
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- dispatch
+
+template <class G, int S>
+__device__ __forceinline__ void run_kind_small(unsigned char *region, const BatchItem &it,
+                                               const BatchSeg &sg)
+{
+    using T = typename G::T;
+    const cx<T> *gin = reinterpret_cast<const cx<T> *>(sg.in) + it.v0 * G::V;
+    cx<T> *gout = reinterpret_cast<cx<T> *>(sg.out) + it.v0 * G::V;
+    batch_passes<G, S>(reinterpret_cast<cx<T> *>(region), it.nv, gout, (T)sg.scale);
+    (void)gin;
+}
+
+template <class G>
+__device__ __forceinline__ void load_kind(unsigned char *region, const BatchItem &it,
+                                          const BatchSeg &sg)
+{
+    using T = typename G::T;
+    const cx<T> *gin = reinterpret_cast<const cx<T> *>(sg.in) + it.v0 * G::V;
+    batch_load<G>(reinterpret_cast<cx<T> *>(region), gin, it.nv * G::V);
+}
+
+template <int N0, int N1, int N2, typename T, int BIG>
+__device__ __forceinline__ void load_kind_any(unsigned char *region, const BatchItem &it,
+                                              const BatchSeg &sg)
+{
+    if constexpr (BIG == 0) load_kind<Geom<N0, N1, N2, T>>(region, it, sg);
+}
+
+template <int N0, int N1, int N2, typename T, int S, int BIG>
+__device__ __forceinline__ void run_kind_any(unsigned char *region, const BatchItem &it,
+                                             const BatchSeg &sg, unsigned char *scratch)
+{
+    if constexpr (BIG > 0) {
+        constexpr long long V = (long long)N0 * N1 * N2;
+        const cx<T> *gin = reinterpret_cast<const cx<T> *>(sg.in) + it.v0 * V;
+        cx<T> *gout = reinterpret_cast<cx<T> *>(sg.out) + it.v0 * V;
+        big_cube<N0, T, S, BIG>(reinterpret_cast<cx<T> *>(region), gin, gout,
+                                reinterpret_cast<cx<T> *>(scratch), (T)sg.scale);
+    } else {
+        run_kind_small<Geom<N0, N1, N2, T>, S>(region, it, sg);
+    }
+}
+
+// Issue the loads of an item (two-phase cubes load inside run_item).
+__device__ __forceinline__ void issue_item_load(unsigned char *region, const BatchItem &it, const BatchSeg &sg)
+{
+    switch (it.kind) {
+#define FFT3D_BK_LOAD(ID, N0, N1, N2, T, S, VPC, SOLO, BIG) \
+    case ID: load_kind_any<N0, N1, N2, T, BIG>(region, it, sg); break;
+        FFT3D_BATCH_KINDS(FFT3D_BK_LOAD)
+#undef FFT3D_BK_LOAD
+    default: break;
+    }
+}
+
+__device__ __forceinline__ void run_item(unsigned char *region, const BatchItem &it, const BatchSeg &sg,
+                         unsigned char *scratch_bytes)
+{
+    switch (it.kind) {
+#define FFT3D_BK_RUN(ID, N0, N1, N2, T, S, VPC, SOLO, BIG) \
+    case ID: run_kind_any<N0, N1, N2, T, S, BIG>(region, it, sg, scratch_bytes); break;
+        FFT3D_BATCH_KINDS(FFT3D_BK_RUN)
+#undef FFT3D_BK_RUN
+    default: break;
+    }
+}
+
+__global__ void __launch_bounds__(BATCH_THREADS, 1)
+    k_batch(const BatchItem *__restrict__ items, int nitems, const BatchSeg *__restrict__ segs,
+            unsigned int *ticket, unsigned char *scratch, long long scratch_per_cta,
+            const unsigned char *__restrict__ solo_of_kind, int *err)
+{
+    extern __shared__ __align__(128) unsigned char smraw[];
+    __shared__ int s_next;
+    (void)err;
+    const int tid = threadIdx.x;
+    unsigned char *my_scratch = scratch ? scratch + (long long)blockIdx.x * scratch_per_cta : nullptr;
+
+    if (tid == 0) s_next = (int)atomicAdd(ticket, 1u);
+    __syncthreads();
+    int cur = s_next;
+    int off = 0;  // byte offset of the current item's region
+    if (cur < nitems) {
+        const BatchItem it = items[cur];
+        issue_item_load(smraw, it, segs[it.seg]);
+    }
+    while (cur < nitems) {
+        const BatchItem it = items[cur];
+        const bool solo = solo_of_kind[it.kind] != 0;
+        __syncthreads();
+        if (tid == 0) s_next = (int)atomicAdd(ticket, 1u);
+        __syncthreads();
+        const int next = s_next;
+        bool pre = false;
+        int noff = 0;
+        if (!solo && next < nitems) {
+            const BatchItem nt = items[next];
+            if (!solo_of_kind[nt.kind]) {
+                pre = true;
+                noff = off == 0 ? BATCH_HALF : 0;
+                issue_item_load(smraw + noff, nt, segs[nt.seg]);
+            }
+        }
+        if (pre) cp_async_wait<1>();
+        else cp_async_wait<0>();
+        __syncthreads();
+        run_item(smraw + off, it, segs[it.seg], my_scratch);
+        __syncthreads();
+        if (!pre && next < nitems) {
+            const BatchItem nt = items[next];
+            noff = 0;
+            issue_item_load(smraw, nt, segs[nt.seg]);
+        }
+        cur = next;
+        off = noff;
+    }
+    cp_async_wait<0>();
+}
+
+const void *batch_kernel_func() { return (const void *)&k_batch; }
+int batch_kernel_threads() { return BATCH_THREADS; }
+int batch_kernel_smem() { return BATCH_SMEM; }
+int batch_kernel_half() { return BATCH_HALF; }
+
+}  // namespace fft3d

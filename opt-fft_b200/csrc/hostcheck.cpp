@@ -78,7 +78,46 @@ static void emulate_cluster(const void *vin, void *vout, long long nvol)
     }
 }
 
+// The batch kernel's two-phase cube: x-slabs (z, y passes) to scratch, then
+// y-slabs from scratch through the x pass (batch_kernel.cu big_cube).
+template <int L, typename T, int S, int PL>
+static void emulate_big_cube(const void *vin, void *vout, long long nvol)
+{
+    constexpr int NS = L / PL;
+    using XG = Geom<PL, L, L, T>;
+    using YG = Geom<L, PL, L, T>;
+    constexpr long long V = (long long)L * L * L;
+    const T scale = S > 0 ? T(1) / T(V) : T(1);
+    std::vector<cx<T>> sm((size_t)(XG::PV > YG::PV ? XG::PV : YG::PV));
+    std::vector<cx<T>> scratch((size_t)V);
+    for (long long vol = 0; vol < nvol; ++vol) {
+        const cx<T> *gin = (const cx<T> *)vin + vol * V;
+        cx<T> *gout = (cx<T> *)vout + vol * V;
+        for (int s = 0; s < NS; ++s) {
+            for (auto &e : sm) e = {T(12345.0), T(-6789.0)};
+            for (int g = 0; g < PL * L * L; ++g)
+                sm[XG::off(g / L, g % L)] = gin[(long long)s * PL * L * L + g];
+            for (int r = 0; r < PL * L; ++r) pass_z<XG, S, ALG_DEFAULT>(sm.data(), r);
+            for (int l = 0; l < PL * L; ++l) pass_y<XG, S, ALG_DEFAULT>(sm.data(), l);
+            for (int g = 0; g < PL * L * L; ++g)
+                scratch[(size_t)s * PL * L * L + g] = sm[XG::off(g / L, g % L)];
+        }
+        for (int s = 0; s < NS; ++s) {
+            for (auto &e : sm) e = {T(12345.0), T(-6789.0)};
+            for (int g = 0; g < L * PL * L; ++g) {
+                const int z = g % L, row = g / L, x = row / PL, yl = row % PL;
+                sm[YG::off(row, z)] = scratch[((size_t)x * L + s * PL + yl) * L + z];
+            }
+            for (int l = 0; l < PL * L; ++l) pass_x_slab<YG, S, L>(sm.data(), l, gout, s * PL, scale);
+        }
+    }
+}
+
 typedef void (*emu_fn)(const void *, void *, long long);
+
+#define EMU_BIG(L, T, PL)                                                               \
+    {L, L, L, sizeof(T) == 8 ? 0 : 1, -1, 200 + PL, 1, &emulate_big_cube<L, T, -1, PL>}, \
+    {L, L, L, sizeof(T) == 8 ? 0 : 1, +1, 200 + PL, 1, &emulate_big_cube<L, T, +1, PL>}
 
 #define EMU_CL(N0, N1, N2, T, C)                                                             \
     {N0, N1, N2, sizeof(T) == 8 ? 0 : 1, -1, 100 + C, 1,                                   \
@@ -108,6 +147,7 @@ static const EmuEntry kEmu[] = {
     EMU(1, 1, 1, double, 0, 1),    EMU(3, 3, 3, double, 0, 1),     EMU(17, 2, 2, double, 0, 1),
     EMU_CL(36, 36, 36, double, 4), EMU_CL(36, 36, 36, double, 6),  EMU_CL(36, 36, 36, double, 9),
     EMU_CL(36, 36, 36, float, 2),  EMU_CL(36, 36, 36, float, 4),   EMU_CL(36, 36, 36, float, 6),
+    EMU_BIG(36, double, 9),        EMU_BIG(36, float, 12),
 };
 
 extern "C" int hostcheck_fft3d(int n0, int n1, int n2, int prec, int sign, int alg, int vpc,

@@ -121,6 +121,27 @@ FFT_HD void pass_x_out(const cx<typename G::T> *sm, int l, cx<typename G::T> *go
     }
 }
 
+// Pass along x over a y-slab held as an (N0, YS, N2) block G, written into a
+// volume whose y extent is GN1, at y offset y0 (two-phase large cubes).
+template <class G, int S, int GN1>
+FFT_HD void pass_x_slab(const cx<typename G::T> *sm, int l, cx<typename G::T> *gvol, int y0,
+                        typename G::T scale)
+{
+    using T = typename G::T;
+    const int z = l % G::N2;
+    const int y = l / G::N2;  // 0 .. YS-1
+    cx<T> v[G::N0];
+#pragma unroll
+    for (int j = 0; j < G::N0; ++j) v[j] = sm[G::off(j * G::N1 + y, z)];
+    dft<G::N0, S, T>(v);
+#pragma unroll
+    for (int j = 0; j < G::N0; ++j) {
+        cx<T> r = v[j];
+        if constexpr (S > 0) r = cscale(r, scale);
+        store_out(gvol + ((long long)j * GN1 + y0 + y) * G::N2 + z, r);
+    }
+}
+
 // Copy element g (in [0, nv*V)) of the CTA's input slice into its layout slot.
 template <class G>
 FFT_HD void stage_in(cx<typename G::T> *sm, const cx<typename G::T> *gin, int g)

@@ -1,0 +1,156 @@
+"""The descriptor-list batch: one persistent launch over segments of uneven
+geometry, both precisions and both directions (needs a B200).
+
+Checks every compiled kind against the oracle, the full uneven complex64 mix of
+the batching configuration (6^3 x 8192 ... 36^3 x 64, 8x8x16 x 1024, with a
+seeded 10% of volumes at log-uniform magnitudes 1e-2..1e2) against the FP64
+oracle per volume, and that every volume's result is bit-identical alone and in
+the mix, with and without CUDA-graph replay.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import field
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+import fft3d_b200 as fb  # noqa: E402
+
+KINDS = [(6, 6, 6), (8, 8, 8), (12, 12, 12), (16, 16, 16), (17, 17, 17), (24, 24, 24),
+         (36, 36, 36), (8, 8, 16), (16, 16, 32)]
+C64_TOL = 2e-6
+C128_TOL = 1e-13
+
+# the batching configuration: (shape, volumes)
+MIX = [((6, 6, 6), 8192), ((8, 8, 8), 4096), ((12, 12, 12), 2048), ((16, 16, 16), 1024),
+       ((17, 17, 17), 512), ((24, 24, 24), 256), ((36, 36, 36), 64), ((8, 8, 16), 1024)]
+
+
+def mix_field(rng, shape, n, dtype):
+    """uniform[-1,1) re/im, except a seeded 10% of volumes with log-uniform
+    magnitudes in [1e-2, 1e2] and uniform phase."""
+    x = field(rng, (n,) + shape, "uniform", np.complex128)
+    tail = rng.random(n) < 0.10
+    k = int(tail.sum())
+    if k:
+        mag = 10.0 ** rng.uniform(-2.0, 2.0, (k,) + shape)
+        ph = rng.uniform(0, 2 * np.pi, (k,) + shape)
+        x[tail] = mag * np.exp(1j * ph)
+    return x.astype(dtype)
+
+
+def make_batch(specs, flags=0):
+    """specs: list of (shape, x numpy, direction, precision).  Returns batch,
+    device inputs and device outputs."""
+    ins, outs, segs = [], [], []
+    for shape, x, d, p in specs:
+        xi = torch.from_numpy(np.ascontiguousarray(x)).cuda()
+        xo = torch.empty_like(xi)
+        ins.append(xi)
+        outs.append(xo)
+        segs.append({"shape": shape, "batch": x.shape[0], "direction": d, "precision": p,
+                     "in": xi.data_ptr(), "out": xo.data_ptr()})
+    return fb.Batch(segs, flags=flags), ins, outs
+
+
+def ref(x, d):
+    x64 = x.astype(np.complex128)
+    return oracle.fft3d(x64) if d == fb.FORWARD else oracle.ifft3d(x64)
+
+
+def test_every_kind_both_precisions_and_directions():
+    rng = np.random.default_rng(5)
+    specs = []
+    for shape in KINDS:
+        v = int(np.prod(shape))
+        n = max(2, min(23, 200000 // v))
+        for p in (fb.C128, fb.C64):
+            for d in (fb.FORWARD, fb.BACKWARD):
+                dt = np.complex128 if p == fb.C128 else np.complex64
+                specs.append((shape, field(rng, (n,) + shape, "normal", dt), d, p))
+    b, ins, outs = make_batch(specs)
+    b.execute()
+    torch.cuda.synchronize()
+    for (shape, x, d, p), o in zip(specs, outs):
+        err = oracle.rel_error_per_volume(o.cpu().numpy().astype(np.complex128), ref(x, d))
+        tol = C128_TOL if p == fb.C128 else C64_TOL
+        assert err.max() < tol, (shape, p, d, err.max())
+
+
+def test_uneven_complex64_mix_against_fp64_oracle():
+    rng = np.random.default_rng(2024)
+    specs = [(shape, mix_field(rng, shape, n, np.complex64), fb.FORWARD, fb.C64) for shape, n in MIX]
+    b, ins, outs = make_batch(specs)
+    assert "graph" in b.describe().lower()
+    b.execute()
+    torch.cuda.synchronize()
+    worst = 0.0
+    for (shape, x, d, p), o in zip(specs, outs):
+        n = x.shape[0]
+        idx = np.sort(rng.choice(n, size=min(n, 48), replace=False))
+        got = o.cpu().numpy()[idx].astype(np.complex128)
+        err = oracle.rel_error_per_volume(got, ref(x[idx], d))
+        worst = max(worst, float(err.max()))
+        assert err.max() < 1e-6, (shape, err.max())
+    print(f"uneven c64 mix: worst per-volume rel L2 vs FP64 oracle {worst:.3e}")
+
+
+def test_alone_equals_mixed_and_graph_equals_direct():
+    rng = np.random.default_rng(9)
+    specs = []
+    for shape in KINDS:
+        for p in (fb.C128, fb.C64):
+            dt = np.complex128 if p == fb.C128 else np.complex64
+            n = 3 if np.prod(shape) > 10000 else 13
+            specs.append((shape, field(rng, (n,) + shape, "uniform", dt), fb.FORWARD, p))
+    mixed, _, mouts = make_batch(specs)
+    mixed.execute()
+    direct, _, douts = make_batch(specs, flags=fb.FLAG_NO_GRAPH)
+    direct.execute()
+    torch.cuda.synchronize()
+    for k, spec in enumerate(specs):
+        alone, _, aouts = make_batch([spec])
+        alone.execute()
+        torch.cuda.synchronize()
+        assert torch.equal(aouts[0], mouts[k]), f"segment {k} differs alone vs mixed"
+        assert torch.equal(douts[k], mouts[k]), f"segment {k} differs graph vs direct"
+
+
+def test_batch_round_trip_and_repeat():
+    rng = np.random.default_rng(17)
+    shapes = [(8, 8, 8), (17, 17, 17), (36, 36, 36), (16, 16, 32)]
+    xs = [field(rng, (5,) + s, "uniform", np.complex128) for s in shapes]
+    fwd, _, fouts = make_batch([(s, x, fb.FORWARD, fb.C128) for s, x in zip(shapes, xs)])
+    fwd.execute()
+    torch.cuda.synchronize()
+    first = [o.clone() for o in fouts]
+    fwd.execute()
+    torch.cuda.synchronize()
+    for a, b in zip(first, fouts):
+        assert torch.equal(a, b)
+    inv, _, iouts = make_batch([(s, o.cpu().numpy(), fb.BACKWARD, fb.C128)
+                                for s, o in zip(shapes, fouts)])
+    inv.execute()
+    torch.cuda.synchronize()
+    for x, o in zip(xs, iouts):
+        assert oracle.rel_error_per_volume(o.cpu().numpy(), x).max() < C128_TOL
+
+
+def test_batch_rejects_bad_segments():
+    x = torch.zeros(4 * 512, dtype=torch.complex128, device="cuda")
+    y = torch.zeros_like(x)
+    ok = {"shape": (8, 8, 8), "batch": 4, "in": x.data_ptr(), "out": y.data_ptr()}
+    with pytest.raises(fb.Fft3dError) as e:
+        fb.Batch([dict(ok, shape=(7, 7, 7))])
+    assert e.value.status == fb.ERR_UNSUPPORTED
+    with pytest.raises(fb.Fft3dError) as e:
+        fb.Batch([dict(ok, out=x.data_ptr() + 16)])
+    assert e.value.status == fb.ERR_OVERLAP
+    with pytest.raises(fb.Fft3dError) as e:
+        fb.Batch([dict(ok, **{"in": x.data_ptr() + 8})])
+    assert e.value.status == fb.ERR_ALIGN
+    empty = fb.Batch([])
+    empty.execute()
+    torch.cuda.synchronize()

@@ -82,6 +82,21 @@ def test_cluster_data_movement(hostcheck, prec, c, sign):
     assert err < (C128_TOL if prec == 0 else C64_TOL), err
 
 
+@pytest.mark.parametrize("prec,pl", [(0, 9), (1, 12)])
+@pytest.mark.parametrize("sign", [-1, +1])
+def test_two_phase_cube(hostcheck, prec, pl, sign):
+    """The batch kernel's two-phase 36^3 route through scratch (alg = 200 + slab)."""
+    shape = (36, 36, 36)
+    rng = np.random.default_rng(4000 + pl)
+    dt = np.complex128 if prec == 0 else np.complex64
+    x = field(rng, (2,) + shape, dist="normal", dtype=dt)
+    got = run(hostcheck, x, shape, prec, sign, 200 + pl, 1)
+    x64 = x.astype(np.complex128)
+    want = oracle.fft3d(x64) if sign < 0 else oracle.ifft3d(x64)
+    err = oracle.rel_error_per_volume(got, want).max()
+    assert err < (C128_TOL if prec == 0 else C64_TOL), err
+
+
 GOLD = [p for p in sorted(glob.glob(os.path.join(GOLDEN, "vol_*.npz")))]
 
 

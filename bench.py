@@ -399,6 +399,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="roundtrip17", choices=sorted(WORKLOADS))
     ap.add_argument("--no-extra", action="store_true", help="skip the per-L workloads")
+    ap.add_argument("--extras", default="all",
+                    help="comma list of the per-L workloads to run (default all, incl. mixed_c64)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0,
                     help="CPU baseline sample length; 0 skips it")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-pointer measurement")
@@ -475,8 +477,11 @@ def main():
                "path": "fft3d_b200_execute_host_chain, page-locked host buffers"}
 
     workloads = {}
+    extras = EXTRA + ["mixed_c64"] if a.extras == "all" else [e for e in a.extras.split(",") if e]
     if not a.no_extra:
-        for name in EXTRA:
+        for name in extras:
+            if name not in WORKLOADS:
+                continue
             ww = WORKLOADS[name]
             if not fb.supports(ww["shape"], ww["prec"]):
                 workloads[name] = {"supported": False}
@@ -492,7 +497,7 @@ def main():
             del x
             torch.cuda.empty_cache()
 
-    if not a.no_extra:
+    if not a.no_extra and "mixed_c64" in extras:
         workloads["mixed_c64"] = measure_mixed(fb, torch, device, stream, peak, max(5, a.steps // 20),
                                                a.warmup, world)
         torch.cuda.empty_cache()

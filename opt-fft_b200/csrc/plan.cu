@@ -43,6 +43,7 @@ const std::vector<KernelEntry> &registry()
     static std::once_flag once;
     std::call_once(once, [] {
         register_stream_kernels(reg);
+        register_direct_kernels(reg);
         register_kernels(reg);
         register_cluster_kernels(reg);
     });

@@ -51,6 +51,23 @@ FFT_HD void pass_z(cx<typename G::T> *sm, int r)
     for (int j = 0; j < G::N2; ++j) sm[G::off(r, j)] = v[j];
 }
 
+// Pass along z for row r read straight from HBM: rows are contiguous in the
+// input (row r of the CTA's slice starts at element r*N2), so a thread streams
+// its N2 points with back-to-back vector loads and the transform needs no
+// staging copy; the result goes to the shared-memory layout.
+template <class G, int S, int ALG>
+FFT_HD void pass_z_from_global(cx<typename G::T> *sm, const cx<typename G::T> *gin, int r)
+{
+    using T = typename G::T;
+    cx<T> v[G::N2];
+    const cx<T> *p = gin + (long long)r * G::N2;
+#pragma unroll
+    for (int j = 0; j < G::N2; ++j) v[j] = load_in(p + j);
+    dft<G::N2, S, T, ALG>(v);
+#pragma unroll
+    for (int j = 0; j < G::N2; ++j) sm[G::off(r, j)] = v[j];
+}
+
 // Pass along y for line l = (vol*N0 + x)*N2 + z.
 template <class G, int S, int ALG>
 FFT_HD void pass_y(cx<typename G::T> *sm, int l)

@@ -137,6 +137,21 @@ void fft3d_b200_batch_destroy(fft3d_b200_batch *batch);
 
 const char *fft3d_b200_batch_describe(const fft3d_b200_batch *batch);
 
+/* Run the segments as one persistent batch launch on `stream` WITHOUT allocating
+ * any device memory -- no counterpart in the reference.  For callers that may
+ * not call cudaMalloc (an application whose pool allocator owns all device
+ * memory, a latency-critical loop that cannot pay cudaMalloc's implicit
+ * synchronisation, a plugin host that forbids allocation): the descriptor list,
+ * work ticket and error word live in one static device array of about 540 KB
+ * that the library holds on every GPU that loads it.  Limits: at most 256
+ * segments and 16384 work items per call, and no 36^3 segments (their two-phase
+ * route needs more scratch than the array holds); beyond these it returns
+ * FFT3D_B200_ERR_BUDGET and enqueues nothing.  The first call on a device looks
+ * up the array's device address (make it before any stream capture).  Calls
+ * share the array and reset its ticket on their stream, so calls that overlap
+ * on the GPU race: order them (one stream, or events). */
+int fft3d_b200_batch_execute_noalloc(const fft3d_b200_segment *segs, int nseg, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -50,6 +50,18 @@ static const KindInfo *find_kind(int n0, int n1, int n2, int prec, int sign)
     return nullptr;
 }
 
+int batch_kind_of(int n0, int n1, int n2, int precision, int sign, int *vpc, int *big,
+                  long long *vol_elems, int *solo)
+{
+    const KindInfo *k = find_kind(n0, n1, n2, precision, sign);
+    if (!k) return -1;
+    if (vpc) *vpc = k->vpc;
+    if (big) *big = k->big;
+    if (vol_elems) *vol_elems = k->vol_elems;
+    if (solo) *solo = (k->solo || k->big || k->stage_bytes > batch_kernel_half()) ? 1 : 0;
+    return k->id;
+}
+
 }  // namespace fft3d
 
 using namespace fft3d;

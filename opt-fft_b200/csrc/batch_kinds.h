@@ -68,6 +68,12 @@ struct BatchSeg {
 
 constexpr int BATCH_NKINDS = 36;
 
+// Kind lookup for the host side (batch.cu): returns the kind id or -1, and the
+// kind's volumes per item, two-phase flag, volume size, and whether its items
+// need all of shared memory.
+int batch_kind_of(int n0, int n1, int n2, int precision, int sign, int *vpc, int *big,
+                  long long *vol_elems, int *solo);
+
 const void *batch_kernel_func();
 int batch_kernel_threads();
 int batch_kernel_smem();

@@ -76,7 +76,7 @@ EXPORTS = {
                      "fft3d_b200_plan_launches", "fft3d_b200_last_status",
                      "fft3d_b200_status_string", "fft3d_b200_batch_create",
                      "fft3d_b200_batch_execute", "fft3d_b200_batch_destroy",
-                     "fft3d_b200_batch_describe"],
+                     "fft3d_b200_batch_describe", "fft3d_b200_batch_execute_noalloc"],
 }
 
 
@@ -118,6 +118,7 @@ def _load():
         "fft3d_b200_batch_execute": ([vp, vp], i),
         "fft3d_b200_batch_destroy": ([vp], None),
         "fft3d_b200_batch_describe": ([vp], ctypes.c_char_p),
+        "fft3d_b200_batch_execute_noalloc": ([ctypes.POINTER(Segment), i, vp], i),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -230,15 +231,27 @@ def execute_host_chain(plans, x, out=None):
     return out
 
 
+def _segments(segments):
+    arr = (Segment * max(1, len(segments)))()
+    for k, s in enumerate(segments):
+        arr[k] = Segment(s["shape"][0], s["shape"][1], s["shape"][2],
+                         s.get("direction", FORWARD), s.get("precision", C128),
+                         int(s["batch"]), s["in"], s["out"])
+    return arr
+
+
+def batch_execute_noalloc(segments, stream: int = 0):
+    """One persistent batch launch with no device allocation (static scratch);
+    see fft3d_b200_batch_execute_noalloc in include/fft3d_b200.h for the limits."""
+    _check(_lib.fft3d_b200_batch_execute_noalloc(_segments(segments), len(segments),
+                                                 stream or None), "batch_execute_noalloc")
+
+
 class Batch:
     """One persistent launch over segments of uneven geometry (device pointers)."""
 
     def __init__(self, segments, flags=0, device=-1):
-        arr = (Segment * len(segments))()
-        for k, s in enumerate(segments):
-            arr[k] = Segment(s["shape"][0], s["shape"][1], s["shape"][2],
-                             s.get("direction", FORWARD), s.get("precision", C128),
-                             int(s["batch"]), s["in"], s["out"])
+        arr = _segments(segments)
         h = ctypes.c_void_p()
         _check(_lib.fft3d_b200_batch_create(arr, len(segments), flags, device, ctypes.byref(h)),
                "batch_create")

@@ -327,6 +327,83 @@ def measure_mixed(fb, torch, device, stream, peak, steps, warmup, world):
     return out
 
 
+# ------------------------------------------------------------------ serving
+
+def measure_serve(fb, torch, device, n_req=10000, seed=2024):
+    """Continuous-batching server vs one launch per request in FP64, on the seeded
+    serving stream: saturation throughput, then Poisson arrivals at 70% of the
+    batched saturation rate, with p50/p99 submit-to-completion latency.
+    Request data is device-resident and distinct per request (its own input and
+    output ranges of an arena larger than L2), so every request is served from
+    HBM; the FP64 baseline gets the same requests in complex128."""
+    from fft3d_b200.workloads import SIDES, request_stream
+    reqs = request_stream(n_req, rate_hz=1.0, seed=seed)
+    sizes =[r["batch"] * int(np.prod(r["shape"])) for r in reqs]
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    total = int(off[-1])
+    a128 = torch.empty(total, dtype=torch.complex128, device=device)
+    a128.real.uniform_(-1, 1)
+    a128.imag.uniform_(-1, 1)
+    o128 = torch.empty_like(a128)
+    a64 = a128.to(torch.complex64)
+    o64 = torch.empty_like(a64)
+
+    def seg_of(r, p, k):
+        src, dst = (a128, o128) if p == 0 else (a64, o64)
+        eb = 16 if p == 0 else 8
+        return {"shape": r["shape"], "batch": r["batch"], "direction": r["direction"],
+                "precision": p, "in": src.data_ptr() + int(off[k]) * eb,
+                "out": dst.data_ptr() + int(off[k]) * eb}
+
+    def run(flags, rate, force_c128, inflight):
+        # requests are submitted by the library's C load generator at their
+        # arrival times, so the client is never the bottleneck
+        srv = fb.Server(64 << 30, max_inflight=inflight, flags=flags)
+        segs = [seg_of(r, 0 if force_c128 else r["precision"], k) for k, r in enumerate(reqs)]
+        arrivals = None
+        if rate:
+            gaps = np.random.default_rng(seed + 2).exponential(1.0 / rate, len(reqs))
+            arrivals = np.cumsum(gaps) - gaps[0]
+        srv.submit_many(segs, arrivals)
+        srv.drain(600)
+        st = srv.stats()
+        srv.close()
+        return st
+
+    # warm-up: every kind and volume-count class once (tuning, first launches)
+    warm = []
+    for L in SIDES:
+        for d in (-1, 1):
+            for p in (0, 1):
+                for b in (1, 2, 4, 8, 16, 32, 64):
+                    warm.append({"shape": (L, L, L), "batch": b, "direction": d, "precision": p})
+    for flags, inflight in ((0, 4), (fb.SERVE_PLAIN, 32)):
+        srv = fb.Server(64 << 30, max_inflight=inflight, flags=flags)
+        for k, r in enumerate(warm):
+            srv.submit(seg_of(r, r["precision"], k))
+        srv.drain(600)
+        srv.close()
+    torch.cuda.synchronize()
+
+    out = {"label": f"{n_req} requests of the seeded serving stream, device-resident data, "
+                    "64 GB admission budget"}
+    sat = run(0, None, False, 4)
+    lam = 0.7 * sat["requests"] / sat["span_s"]
+    pois = run(0, lam, False, 4)
+    psat = run(fb.SERVE_PLAIN, None, True, 32)
+    ppois = run(fb.SERVE_PLAIN, lam, True, 32)
+    keep = ("volumes_per_s", "p50_s", "p99_s", "mean_requests_per_launch", "launches")
+    out["batched_saturation"] = {k: sat[k] for k in keep}
+    out["batched_poisson"] = dict({k: pois[k] for k in keep}, arrival_rate_hz=lam)
+    out["plain_fp64_saturation"] = {k: psat[k] for k in keep}
+    out["plain_fp64_poisson"] = dict({k: ppois[k] for k in keep}, arrival_rate_hz=lam)
+    out["throughput_ratio_saturation"] = sat["volumes_per_s"] / psat["volumes_per_s"]
+    out["bytes_in_per_run"] = int(sum(s * (16 if r["precision"] == 0 else 8)
+                                      for s, r in zip(sizes, reqs)))
+    del a128, o128, a64, o64
+    return out
+
+
 # ------------------------------------------------------------------ CPU reference
 
 def aligned(shape, dtype=np.complex128, align=64):
@@ -477,7 +554,7 @@ def main():
                "path": "fft3d_b200_execute_host_chain, page-locked host buffers"}
 
     workloads = {}
-    extras = EXTRA + ["mixed_c64"] if a.extras == "all" else [e for e in a.extras.split(",") if e]
+    extras = EXTRA + ["mixed_c64", "serve"] if a.extras == "all" else [e for e in a.extras.split(",") if e]
     if not a.no_extra:
         for name in extras:
             if name not in WORKLOADS:
@@ -500,6 +577,9 @@ def main():
     if not a.no_extra and "mixed_c64" in extras:
         workloads["mixed_c64"] = measure_mixed(fb, torch, device, stream, peak, max(5, a.steps // 20),
                                                a.warmup, world)
+        torch.cuda.empty_cache()
+    if not a.no_extra and "serve" in extras and world == 1:
+        workloads["serve"] = measure_serve(fb, torch, device)
         torch.cuda.empty_cache()
 
     cpu = None

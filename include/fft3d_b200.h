@@ -137,6 +137,55 @@ void fft3d_b200_batch_destroy(fft3d_b200_batch *batch);
 
 const char *fft3d_b200_batch_describe(const fft3d_b200_batch *batch);
 
+/* ---------------------------------------------------------------- serving */
+
+typedef struct fft3d_b200_server fft3d_b200_server;
+
+#define FFT3D_B200_SERVE_PLAIN 0x1u /* baseline: one launch per request, no coalescing */
+
+typedef struct {
+    long long requests;         /* finished */
+    long long volumes;          /* finished */
+    long long launches;         /* batch launches (plain mode: request launches) */
+    double mean_requests_per_launch;
+    long long peak_admitted_bytes; /* high-water mark of admitted in+out bytes */
+    double p50_s, p99_s, mean_s, max_s; /* submit-to-completion latency */
+    double volumes_per_s;       /* finished volumes / (last completion - first submission) */
+    double span_s;
+} fft3d_b200_server_stats;
+
+/* Start a continuous-batching server on `device`: requests (segments with device
+ * in/out pointers) are admitted while the in+out bytes of unfinished requests
+ * stay within `hbm_budget_bytes`, coalesced into persistent batch launches on up
+ * to `max_inflight` concurrent streams, and completed asynchronously. */
+int fft3d_b200_server_create(size_t hbm_budget_bytes, int max_inflight, unsigned flags, int device,
+                             fft3d_b200_server **out);
+
+/* Queue one request (thread-safe).  FFT3D_B200_ERR_BUDGET if it alone exceeds
+ * the budget.  `ticket` identifies it in fft3d_b200_server_poll. */
+int fft3d_b200_server_submit(fft3d_b200_server *server, const fft3d_b200_segment *request,
+                             unsigned long long *ticket);
+
+/* Load generator: submit requests[k] at arrival_s[k] seconds after the call
+ * starts (busy-waiting between arrivals; NULL arrival_s = all at once), from the
+ * calling thread.  Returns after the last submission; tickets (optional) get the
+ * request tickets.  Stops at the first refused request and returns its status. */
+int fft3d_b200_server_submit_many(fft3d_b200_server *server, const fft3d_b200_segment *requests,
+                                  const double *arrival_s, int n, unsigned long long *tickets);
+
+/* Tickets of requests finished since the last poll, in completion order; returns
+ * how many were written (<= max). */
+int fft3d_b200_server_poll(fft3d_b200_server *server, unsigned long long *tickets, int max);
+
+/* Wait until every submitted request has finished (FFT3D_B200_ERR_TIMEOUT after
+ * `timeout_s` seconds). */
+int fft3d_b200_server_drain(fft3d_b200_server *server, double timeout_s);
+
+/* Latency percentiles and throughput of everything finished so far. */
+int fft3d_b200_server_get_stats(fft3d_b200_server *server, fft3d_b200_server_stats *stats);
+
+void fft3d_b200_server_destroy(fft3d_b200_server *server);
+
 /* Run the segments as one persistent batch launch on `stream` WITHOUT allocating
  * any device memory -- no counterpart in the reference.  For callers that may
  * not call cudaMalloc (an application whose pool allocator owns all device

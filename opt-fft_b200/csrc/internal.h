@@ -55,4 +55,9 @@ int entry_occupancy(const KernelEntry &e, int device);
 
 int element_bytes(int precision);
 
+// The autotuner's choice for a geometry at a batch size (memoised per batch
+// bucket like plan creation); nullptr if the geometry has no kernel.
+const KernelEntry *tuned_entry(int device, int n0, int n1, int n2, int precision, int sign,
+                               long long batch);
+
 }  // namespace fft3d

@@ -260,6 +260,25 @@ static const KernelEntry *tune(const std::vector<const KernelEntry *> &cands, in
     return best ? best : cands[0];
 }
 
+const KernelEntry *tuned_entry(int device, int n0, int n1, int n2, int precision, int sign,
+                               long long batch)
+{
+    auto cands = candidates(n0, n1, n2, precision, sign);
+    if (cands.empty()) return nullptr;
+    auto key = std::make_tuple(device, n0, n1, n2, precision, sign, batch_bucket(batch));
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) return it->second;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    const KernelEntry *k =
+        getenv("FFT3D_B200_NO_TUNE")
+            ? cands[0]
+            : tune(cands, device, batch, precision, (long long)n0 * n1 * n2, sms, nullptr, nullptr);
+    g_tuned[key] = k;
+    return k;
+}
+
 }  // namespace fft3d
 
 using namespace fft3d;

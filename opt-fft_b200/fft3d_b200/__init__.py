@@ -62,6 +62,16 @@ class Segment(ctypes.Structure):
                 ("batch", ctypes.c_longlong), ("in_", ctypes.c_void_p), ("out", ctypes.c_void_p)]
 
 
+class ServerStats(ctypes.Structure):
+    _fields_ = [("requests", ctypes.c_longlong), ("volumes", ctypes.c_longlong),
+                ("launches", ctypes.c_longlong), ("mean_requests_per_launch", ctypes.c_double),
+                ("peak_admitted_bytes", ctypes.c_longlong), ("p50_s", ctypes.c_double),
+                ("p99_s", ctypes.c_double), ("mean_s", ctypes.c_double), ("max_s", ctypes.c_double),
+                ("volumes_per_s", ctypes.c_double), ("span_s", ctypes.c_double)]
+
+
+SERVE_PLAIN = 0x1
+
 # Every symbol the headers in include/ declare, by header.
 EXPORTS = {
     "fft3d_api.h": ["fft3d_name", "fft3d_description", "fft3d_supports", "fft3d_create",
@@ -76,7 +86,11 @@ EXPORTS = {
                      "fft3d_b200_plan_launches", "fft3d_b200_last_status",
                      "fft3d_b200_status_string", "fft3d_b200_batch_create",
                      "fft3d_b200_batch_execute", "fft3d_b200_batch_destroy",
-                     "fft3d_b200_batch_describe", "fft3d_b200_batch_execute_noalloc"],
+                     "fft3d_b200_batch_describe", "fft3d_b200_batch_execute_noalloc",
+                     "fft3d_b200_server_create", "fft3d_b200_server_submit",
+                     "fft3d_b200_server_submit_many",
+                     "fft3d_b200_server_poll", "fft3d_b200_server_drain",
+                     "fft3d_b200_server_get_stats", "fft3d_b200_server_destroy"],
 }
 
 
@@ -119,6 +133,16 @@ def _load():
         "fft3d_b200_batch_destroy": ([vp], None),
         "fft3d_b200_batch_describe": ([vp], ctypes.c_char_p),
         "fft3d_b200_batch_execute_noalloc": ([ctypes.POINTER(Segment), i, vp], i),
+        "fft3d_b200_server_create": ([ctypes.c_size_t, i, ctypes.c_uint, i, ctypes.POINTER(vp)], i),
+        "fft3d_b200_server_submit": ([vp, ctypes.POINTER(Segment),
+                                      ctypes.POINTER(ctypes.c_ulonglong)], i),
+        "fft3d_b200_server_submit_many": ([vp, ctypes.POINTER(Segment),
+                                           ctypes.POINTER(ctypes.c_double), i,
+                                           ctypes.POINTER(ctypes.c_ulonglong)], i),
+        "fft3d_b200_server_poll": ([vp, ctypes.POINTER(ctypes.c_ulonglong), i], i),
+        "fft3d_b200_server_drain": ([vp, ctypes.c_double], i),
+        "fft3d_b200_server_get_stats": ([vp, ctypes.POINTER(ServerStats)], i),
+        "fft3d_b200_server_destroy": ([vp], None),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -266,6 +290,64 @@ class Batch:
     def close(self):
         if getattr(self, "_h", None):
             _lib.fft3d_b200_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching request server (fft3d_b200_server_*).
+
+    Requests are segment dicts (shape, batch, direction, precision, device in/out
+    pointers).  They are admitted against `budget_bytes` of in+out HBM, coalesced
+    into persistent batch launches on up to `max_inflight` streams, and finish
+    asynchronously; `stats()` gives p50/p99 latency and throughput."""
+
+    def __init__(self, budget_bytes, max_inflight=4, flags=0, device=-1):
+        h = ctypes.c_void_p()
+        _check(_lib.fft3d_b200_server_create(int(budget_bytes), max_inflight, flags, device,
+                                             ctypes.byref(h)), "server_create")
+        self._h = h
+
+    def submit(self, seg) -> int:
+        arr = _segments([seg])
+        t = ctypes.c_ulonglong()
+        _check(_lib.fft3d_b200_server_submit(self._h, arr, ctypes.byref(t)), "server_submit")
+        return t.value
+
+    def submit_many(self, segs, arrival_s=None):
+        """Submit segs[k] at arrival_s[k] seconds from now (C load generator)."""
+        arr = _segments(segs)
+        times = None
+        if arrival_s is not None:
+            times = (ctypes.c_double * len(segs))(*[float(t) for t in arrival_s])
+        tk = (ctypes.c_ulonglong * max(1, len(segs)))()
+        _check(_lib.fft3d_b200_server_submit_many(self._h, arr, times, len(segs), tk),
+               "server_submit_many")
+        return [tk[k] for k in range(len(segs))]
+
+    def poll(self, max_n=4096):
+        buf = (ctypes.c_ulonglong * max_n)()
+        n = _lib.fft3d_b200_server_poll(self._h, buf, max_n)
+        if n < 0:
+            raise Fft3dError(n, "server_poll")
+        return [buf[k] for k in range(n)]
+
+    def drain(self, timeout_s=120.0):
+        _check(_lib.fft3d_b200_server_drain(self._h, float(timeout_s)), "server_drain")
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(_lib.fft3d_b200_server_get_stats(self._h, ctypes.byref(st)), "server_stats")
+        return {name: getattr(st, name) for name, _ in ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.fft3d_b200_server_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -86,3 +86,9 @@ def test_no_cpu_fallback_without_gpu():
     with pytest.raises(fb.Fft3dError) as e:
         fb.Plan((8, 8, 8), 4)
     assert e.value.status == fb.ERR_CUDA
+    with pytest.raises(fb.Fft3dError) as e:
+        fb.Server(1 << 30)
+    assert e.value.status == fb.ERR_CUDA
+    with pytest.raises(fb.Fft3dError) as e:
+        fb.Batch([])
+    assert e.value.status == fb.ERR_CUDA

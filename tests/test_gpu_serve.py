@@ -1,0 +1,121 @@
+"""The continuous-batching server (needs a B200).
+
+A seeded stream of mixed requests (geometry, volume count, direction,
+precision) goes through fft3d_b200_server_*: every result is checked against the
+oracle, every result is bit-identical to the same request run alone, the HBM
+admission budget is never exceeded, oversize requests are refused, and the
+one-launch-per-request baseline mode gives the same answers.
+"""
+import time
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import field
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+import fft3d_b200 as fb  # noqa: E402
+from fft3d_b200.workloads import request_stream  # noqa: E402
+
+C128_TOL = 1e-13
+C64_TOL = 2e-6
+
+
+def materialise(reqs, seed=1):
+    rng = np.random.default_rng(seed)
+    out = []
+    for r in reqs:
+        dt = np.complex128 if r["precision"] == fb.C128 else np.complex64
+        x = field(rng, (r["batch"],) + r["shape"], "uniform", dt)
+        xi = torch.from_numpy(x).cuda()
+        out.append((r, x, xi, torch.full_like(xi, complex(3.0, 3.0))))
+    return out
+
+
+def seg(r, xi, xo):
+    return {"shape": r["shape"], "batch": r["batch"], "direction": r["direction"],
+            "precision": r["precision"], "in": xi.data_ptr(), "out": xo.data_ptr()}
+
+
+def ref(x, d):
+    x64 = x.astype(np.complex128)
+    return oracle.fft3d(x64) if d == fb.FORWARD else oracle.ifft3d(x64)
+
+
+@pytest.mark.parametrize("flags", [0, fb.SERVE_PLAIN])
+def test_stream_results_match_oracle_and_alone(flags):
+    reqs = [r for r in request_stream(160, rate_hz=4000.0, seed=7)]
+    # keep the test fast: cap the 36^3 requests' volume counts
+    for r in reqs:
+        if r["shape"][0] >= 24:
+            r["batch"] = min(r["batch"], 3)
+    work = materialise(reqs)
+    srv = fb.Server(budget_bytes=64 << 30, max_inflight=4, flags=flags)
+    t0 = time.perf_counter()
+    tickets = []
+    for r, x, xi, xo in work:
+        while time.perf_counter() - t0 < r["t"]:
+            pass
+        tickets.append(srv.submit(seg(r, xi, xo)))
+    srv.drain(120)
+    done = []
+    while True:
+        got = srv.poll()
+        if not got:
+            break
+        done += got
+    assert sorted(done) == sorted(tickets)
+    st = srv.stats()
+    assert st["requests"] == len(reqs)
+    assert st["p99_s"] >= st["p50_s"] > 0
+    if flags == 0:
+        assert st["launches"] <= len(reqs)
+    srv.close()
+    torch.cuda.synchronize()
+    for r, x, xi, xo in work:
+        got = xo.cpu().numpy()
+        err = oracle.rel_error_per_volume(got.astype(np.complex128), ref(x, r["direction"]))
+        tol = C128_TOL if r["precision"] == fb.C128 else C64_TOL
+        assert err.max() < tol, (r, err.max())
+    if flags == 0:
+        # each result is the same alone as in the mix
+        for r, x, xi, xo in work[:40]:
+            alone = torch.empty_like(xo)
+            b = fb.Batch([seg(r, xi, alone)])
+            b.execute()
+            torch.cuda.synchronize()
+            assert torch.equal(alone, xo), r
+            b.close()
+
+
+def test_admission_budget_and_refusals():
+    rng = np.random.default_rng(3)
+    reqs = []
+    for k in range(24):
+        x = field(rng, (8, 17, 17, 17), "uniform", np.complex128)
+        xi = torch.from_numpy(x).cuda()
+        reqs.append((x, xi, torch.empty_like(xi)))
+    one = 2 * 8 * 17 ** 3 * 16
+    srv = fb.Server(budget_bytes=int(2.5 * one), max_inflight=8)
+    for x, xi, xo in reqs:
+        srv.submit({"shape": (17, 17, 17), "batch": 8, "in": xi.data_ptr(), "out": xo.data_ptr()})
+    srv.drain(60)
+    st = srv.stats()
+    assert st["requests"] == len(reqs)
+    assert st["peak_admitted_bytes"] <= int(2.5 * one)
+    torch.cuda.synchronize()
+    for x, xi, xo in reqs:
+        assert oracle.rel_error_per_volume(xo.cpu().numpy(), oracle.fft3d(x)).max() < C128_TOL
+    # a request larger than the whole budget is refused
+    big = torch.zeros(64 * 36 ** 3, dtype=torch.complex128, device="cuda")
+    bo = torch.zeros_like(big)
+    with pytest.raises(fb.Fft3dError) as e:
+        srv.submit({"shape": (36, 36, 36), "batch": 64, "in": big.data_ptr(), "out": bo.data_ptr()})
+    assert e.value.status == fb.ERR_BUDGET
+    with pytest.raises(fb.Fft3dError) as e:
+        srv.submit({"shape": (7, 7, 7), "batch": 1, "in": big.data_ptr(), "out": bo.data_ptr()})
+    assert e.value.status == fb.ERR_UNSUPPORTED
+    srv.close()

@@ -404,6 +404,63 @@ def measure_serve(fb, torch, device, n_req=10000, seed=2024):
     return out
 
 
+# ------------------------------------------------------------------ chains
+
+CHAIN_POINTS = [(6, 64, 4856), (8, 64, 2572), (17, 32, 98)]  # (L, B, m) graded points
+
+
+def measure_chain(fb, torch, device, cpu=True):
+    """The reference's graded map chain z = FFT(x)+c; x <- z/(1+|z|) at its
+    fixed points: one launch per chain on the GPU, against the reference's own
+    single-threaded chain driver (ours_run, bench/geom/best/ours_chain.c) timed on
+    the host.  Unit: transforms/s = B*m / time."""
+    out = {}
+    lib = None
+    path = os.path.join(ROOT, "oracle", "_ref", "libfft3d_best.so")
+    if cpu and os.path.exists(path):
+        lib = ctypes.CDLL(path)
+        lib.ours_setup.argtypes = [ctypes.c_int, ctypes.c_long]
+        lib.ours_run.argtypes = [ctypes.c_int, ctypes.c_long, ctypes.c_long] + [ctypes.c_void_p] * 4
+    for L, B, m in CHAIN_POINTS:
+        rng = np.random.default_rng(L)
+        x = field(rng, (B, L, L, L), "uniform", np.complex128)
+        c = field(rng, (B, L, L, L), "uniform", np.complex128)
+        xi = torch.from_numpy(x).to(device)
+        ci = torch.from_numpy(c).to(device)
+        xo = torch.empty_like(xi)
+        ch = fb.Chain((L, L, L), B, fb.CHAIN_MAP, fb.C128, ci.data_ptr())
+        ch.run(xi.data_ptr(), xo.data_ptr(), m)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        reps = 3
+        e0.record()
+        for _ in range(reps):
+            ch.run(xi.data_ptr(), xo.data_ptr(), m)
+        e1.record()
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / reps * 1e-3
+        res = {"B": B, "m": m, "gpu_s": t, "gpu_transforms_per_s": B * m / t, "launches": 1}
+        if lib is not None:
+            lib.ours_setup(L, B)
+            one = aligned((B, L, L, L))
+            end = aligned((B, L, L, L))
+            xa = aligned((B, L, L, L))
+            ca = aligned((B, L, L, L))
+            xa[...] = x
+            ca[...] = c
+            mm = max(1, min(m, int(m * 0.25)))
+            t0 = time.perf_counter()
+            lib.ours_run(L, B, mm, xa.ctypes.data, ca.ctypes.data, one.ctypes.data, end.ctypes.data)
+            tc = (time.perf_counter() - t0) * m / mm
+            res.update({"cpu_reference_s": tc, "cpu_transforms_per_s": B * m / tc,
+                        "cpu_sample": f"ours_run, 1 thread, {mm} of {m} steps timed, scaled",
+                        "speedup": tc / t})
+        out[f"L{L}_B{B}_m{m}"] = res
+        ch.close()
+    return out
+
+
 # ------------------------------------------------------------------ CPU reference
 
 def aligned(shape, dtype=np.complex128, align=64):
@@ -554,7 +611,8 @@ def main():
                "path": "fft3d_b200_execute_host_chain, page-locked host buffers"}
 
     workloads = {}
-    extras = EXTRA + ["mixed_c64", "serve"] if a.extras == "all" else [e for e in a.extras.split(",") if e]
+    extras = (EXTRA + ["mixed_c64", "chain", "serve"] if a.extras == "all"
+              else [e for e in a.extras.split(",") if e])
     if not a.no_extra:
         for name in extras:
             if name not in WORKLOADS:
@@ -577,6 +635,9 @@ def main():
     if not a.no_extra and "mixed_c64" in extras:
         workloads["mixed_c64"] = measure_mixed(fb, torch, device, stream, peak, max(5, a.steps // 20),
                                                a.warmup, world)
+        torch.cuda.empty_cache()
+    if not a.no_extra and "chain" in extras:
+        workloads["chain"] = measure_chain(fb, torch, device, cpu=(rank == 0 and a.cpu_seconds > 0))
         torch.cuda.empty_cache()
     if not a.no_extra and "serve" in extras and world == 1:
         workloads["serve"] = measure_serve(fb, torch, device)

@@ -137,6 +137,27 @@ void fft3d_b200_batch_destroy(fft3d_b200_batch *batch);
 
 const char *fft3d_b200_batch_describe(const fft3d_b200_batch *batch);
 
+/* ---------------------------------------------------------------- chains */
+
+/* The reference's chain workloads (docs/GRADER.md, bench/geom/best/ours_chain.c:36-53):
+ * m forward transforms, each followed by a pointwise step. */
+#define FFT3D_B200_CHAIN_UNITARY 1 /* state <- FFT(state) * V^(-1/2) */
+#define FFT3D_B200_CHAIN_MAP 2     /* z = FFT(state) + c;  state <- z / (1 + |z|) */
+
+typedef struct fft3d_b200_chain fft3d_b200_chain;
+
+/* A chain over `batch` volumes; for CHAIN_MAP, `d_c` is the constant field
+ * (device pointer, same shape and precision as the state). */
+int fft3d_b200_chain_create(int n0, int n1, int n2, long long batch, int precision, int kind,
+                            const void *d_c, int device, fft3d_b200_chain **out);
+
+/* Run `steps` chain steps from d_x0, leaving the end state in d_out (one launch;
+ * each volume stays in one CTA's shared memory for the whole chain). */
+int fft3d_b200_chain_run(fft3d_b200_chain *chain, const void *d_x0, void *d_out, long long steps,
+                         void *stream);
+
+void fft3d_b200_chain_destroy(fft3d_b200_chain *chain);
+
 /* ---------------------------------------------------------------- serving */
 
 typedef struct fft3d_b200_server fft3d_b200_server;

@@ -30,6 +30,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cmath>
+
 #if defined(__CUDACC__)
 #define FFT_HD __host__ __device__ __forceinline__
 #else

@@ -150,6 +150,44 @@ static const EmuEntry kEmu[] = {
     EMU_BIG(36, double, 9),        EMU_BIG(36, float, 12),
 };
 
+// The chain kernel's per-CTA loop (chain_kernels.cu k_chain) for one volume per CTA.
+template <int N0, int N1, int N2, typename T, int EPI>
+static void emulate_chain(const void *vin, void *vout, const void *vc, long long nvol, long long steps)
+{
+    using G = Geom<N0, N1, N2, T>;
+    const cx<T> *in = (const cx<T> *)vin;
+    const cx<T> *cmap = (const cx<T> *)vc;
+    cx<T> *out = (cx<T> *)vout;
+    const T us = T(1) / std::sqrt(T(G::V));
+    std::vector<cx<T>> sm((size_t)G::PV);
+    for (long long v = 0; v < nvol; ++v) {
+        const long long e0 = v * G::V;
+        for (int g = 0; g < G::V; ++g) stage_in<G>(sm.data(), in + e0, g);
+        for (long long s = 0; s < steps; ++s) {
+            for (int r = 0; r < G::ROWS; ++r) pass_z<G, -1, ALG_DEFAULT>(sm.data(), r);
+            for (int l = 0; l < G::N0 * G::N2; ++l) pass_y<G, -1, ALG_DEFAULT>(sm.data(), l);
+            for (int l = 0; l < G::N1 * G::N2; ++l)
+                pass_x_chain<G, ALG_DEFAULT, EPI>(sm.data(), l, cmap, e0, us);
+        }
+        for (int g = 0; g < G::V; ++g) out[e0 + g] = sm[G::off(g / G::N2, g % G::N2)];
+    }
+}
+
+extern "C" int hostcheck_chain(int n, int prec, int epi, const void *in, void *out, const void *c,
+                               long long nvol, long long steps)
+{
+    ensure_host_tables();
+#define HC_CHAIN(L, T)                                                                          \
+    if (n == L && prec == (sizeof(T) == 8 ? 0 : 1)) {                                          \
+        if (epi == EPI_UNITARY) emulate_chain<L, L, L, T, EPI_UNITARY>(in, out, c, nvol, steps); \
+        else emulate_chain<L, L, L, T, EPI_MAP>(in, out, c, nvol, steps);                       \
+        return 0;                                                                               \
+    }
+    HC_CHAIN(6, double) HC_CHAIN(8, double) HC_CHAIN(17, double) HC_CHAIN(8, float)
+#undef HC_CHAIN
+    return -2;
+}
+
 extern "C" int hostcheck_fft3d(int n0, int n1, int n2, int prec, int sign, int alg, int vpc,
                                const void *in, void *out, long long nvol)
 {

@@ -138,6 +138,46 @@ FFT_HD void pass_x_out(const cx<typename G::T> *sm, int l, cx<typename G::T> *go
     }
 }
 
+// Chain-step epilogues applied to each output point of the last pass.
+constexpr int EPI_UNITARY = 1;  // state <- FFT(state) * V^(-1/2)
+constexpr int EPI_MAP = 2;      // z = FFT(state) + c;  state <- z / (1 + |z|)
+
+template <int EPI, typename T>
+FFT_HD cx<T> chain_epilogue(cx<T> r, const cx<T> *cmap, long long e, T uscale)
+{
+    if constexpr (EPI == EPI_UNITARY) {
+        return cscale(r, uscale);
+    } else {
+        const cx<T> c = cmap[e];
+        const T re = r.re + c.re, im = r.im + c.im;
+        const T s = T(1) / (T(1) + std::sqrt(re * re + im * im));
+        return {re * s, im * s};
+    }
+}
+
+// Pass along x for line l = (vol*N1 + y)*N2 + z with the chain epilogue, result
+// written back into the shared-memory layout (the state stays on chip between
+// chain steps).  `e0` is the global element index of the CTA's first volume.
+template <class G, int ALG, int EPI>
+FFT_HD void pass_x_chain(cx<typename G::T> *sm, int l, const cx<typename G::T> *cmap, long long e0,
+                         typename G::T uscale)
+{
+    using T = typename G::T;
+    const int z = l % G::N2;
+    const int t = l / G::N2;
+    const int y = t % G::N1;
+    const int vol = t / G::N1;
+    cx<T> v[G::N0];
+#pragma unroll
+    for (int j = 0; j < G::N0; ++j) v[j] = sm[G::off((vol * G::N0 + j) * G::N1 + y, z)];
+    dft<G::N0, -1, T, ALG>(v);
+    const long long eb = e0 + (long long)vol * G::V + y * G::N2 + z;
+#pragma unroll
+    for (int j = 0; j < G::N0; ++j)
+        sm[G::off((vol * G::N0 + j) * G::N1 + y, z)] =
+            chain_epilogue<EPI>(v[j], cmap, eb + (long long)j * (G::N1 * G::N2), uscale);
+}
+
 // Pass along x over a y-slab held as an (N0, YS, N2) block G, written into a
 // volume whose y extent is GN1, at y offset y0 (two-phase large cubes).
 template <class G, int S, int GN1>

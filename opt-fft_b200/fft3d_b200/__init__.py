@@ -71,6 +71,8 @@ class ServerStats(ctypes.Structure):
 
 
 SERVE_PLAIN = 0x1
+CHAIN_UNITARY = 1
+CHAIN_MAP = 2
 
 # Every symbol the headers in include/ declare, by header.
 EXPORTS = {
@@ -87,6 +89,8 @@ EXPORTS = {
                      "fft3d_b200_status_string", "fft3d_b200_batch_create",
                      "fft3d_b200_batch_execute", "fft3d_b200_batch_destroy",
                      "fft3d_b200_batch_describe", "fft3d_b200_batch_execute_noalloc",
+                     "fft3d_b200_chain_create", "fft3d_b200_chain_run",
+                     "fft3d_b200_chain_destroy",
                      "fft3d_b200_server_create", "fft3d_b200_server_submit",
                      "fft3d_b200_server_submit_many",
                      "fft3d_b200_server_poll", "fft3d_b200_server_drain",
@@ -133,6 +137,9 @@ def _load():
         "fft3d_b200_batch_destroy": ([vp], None),
         "fft3d_b200_batch_describe": ([vp], ctypes.c_char_p),
         "fft3d_b200_batch_execute_noalloc": ([ctypes.POINTER(Segment), i, vp], i),
+        "fft3d_b200_chain_create": ([i, i, i, ll, i, i, vp, i, ctypes.POINTER(vp)], i),
+        "fft3d_b200_chain_run": ([vp, vp, vp, ll, vp], i),
+        "fft3d_b200_chain_destroy": ([vp], None),
         "fft3d_b200_server_create": ([ctypes.c_size_t, i, ctypes.c_uint, i, ctypes.POINTER(vp)], i),
         "fft3d_b200_server_submit": ([vp, ctypes.POINTER(Segment),
                                       ctypes.POINTER(ctypes.c_ulonglong)], i),
@@ -290,6 +297,33 @@ class Batch:
     def close(self):
         if getattr(self, "_h", None):
             _lib.fft3d_b200_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Chain:
+    """m forward transforms with a pointwise step each (CHAIN_UNITARY or CHAIN_MAP),
+    one launch per run; volumes stay in shared memory for the whole chain."""
+
+    def __init__(self, shape, batch, kind, precision=C128, d_c=0, device=-1):
+        n0, n1, n2 = shape
+        h = ctypes.c_void_p()
+        _check(_lib.fft3d_b200_chain_create(n0, n1, n2, int(batch), precision, kind, d_c or None,
+                                            device, ctypes.byref(h)), "chain_create")
+        self._h = h
+
+    def run(self, d_x0: int, d_out: int, steps: int, stream: int = 0):
+        _check(_lib.fft3d_b200_chain_run(self._h, d_x0, d_out, int(steps), stream or None),
+               "chain_run")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.fft3d_b200_chain_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -43,6 +43,8 @@ const std::vector<KernelEntry> &registry();
 void register_kernels(std::vector<KernelEntry> &out);          // volume_kernels.cu
 void register_stream_kernels(std::vector<KernelEntry> &out);   // stream_kernels.cu
 void register_direct_kernels(std::vector<KernelEntry> &out);   // direct_kernels.cu
+void register_tc_kernels(std::vector<KernelEntry> &out);       // tc_kernels.cu
+int tc_tables_upload();                                         // split-BF16 DFT matrices
 void register_cluster_kernels(std::vector<KernelEntry> &out);  // cluster_kernels.cu
 
 // Launch `e` over `nvol` volumes.  scale multiplies every output (1/V for inverse).

@@ -44,6 +44,7 @@ const std::vector<KernelEntry> &registry()
     std::call_once(once, [] {
         register_stream_kernels(reg);
         register_direct_kernels(reg);
+        register_tc_kernels(reg);
         register_kernels(reg);
         register_cluster_kernels(reg);
     });

@@ -26,6 +26,7 @@ int ensure_device_tables(int device)
         return FFT3D_B200_ERR_CUDA;
     if (cudaMemcpyToSymbol(c_rader17_f, h_rader17_f, sizeof(h_rader17_f)) != cudaSuccess)
         return FFT3D_B200_ERR_CUDA;
+    if (tc_tables_upload() != FFT3D_B200_OK) return FFT3D_B200_ERR_CUDA;
     g_dev_done[device] = true;
     return FFT3D_B200_OK;
 }

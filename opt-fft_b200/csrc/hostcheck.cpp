@@ -11,6 +11,7 @@
 
 #include <vector>
 
+#include "twopass.cuh"
 #include "volume.cuh"
 
 namespace fft3d {
@@ -113,7 +114,70 @@ static void emulate_big_cube(const void *vin, void *vout, long long nvol)
     }
 }
 
+static long long g_twopass_violations = 0;
+
+// The TWOPASS kernel's work items (twopass_kernels.cu k_twopass), taken in
+// ticket order with the kernel's decode, element maps and ring of R slots.
+// Ticket order satisfies every dependency, so one "CTA" can run them in turn;
+// the small grid of 7 CTAs keeps R small, so the ring wraps many times.
+template <int N0, int N1, int N2, typename T, int S, int G>
+static void emulate_twopass(const void *vin, void *vout, long long nvol)
+{
+    using TG = TwoPassGeom<N0, N1, N2, T, G>;
+    using XG = typename TG::XG;
+    using YG = typename TG::YG;
+    const T scale = S > 0 ? T(1) / T(TG::V) : T(1);
+    int lag = 0;
+    const int R = twopass_ring_size(TG::NA, TG::NB, 7, &lag);
+    std::vector<cx<T>> sm((size_t)TG::PV), ring((size_t)R * TG::V, cx<T>{T(-777.0), T(555.0)});
+    const cx<T> *in = (const cx<T> *)vin;
+    cx<T> *out = (cx<T> *)vout;
+    const long long total = (long long)(TG::NA + TG::NB) * nvol;
+    std::vector<long long> cnt_plane(R, 0), cnt_row(R, 0);
+    for (long long t = 0; t < total; ++t) {
+        const TwoPassItem it = twopass_decode(t, nvol, TG::NA, TG::NB, lag);
+        const int slot = (int)(it.vol % R);
+        const long long round = it.vol / R;
+        cx<T> *sv = ring.data() + slot * TG::V;
+        for (auto &e : sm) e = {T(12345.0), T(-6789.0)};
+        // the kernel's waits must already hold in ticket order
+        if (it.plane ? cnt_row[slot] < TG::NB * round : cnt_plane[slot] < TG::NA * (round + 1))
+            g_twopass_violations++;
+        (it.plane ? cnt_plane : cnt_row)[slot]++;
+        if (it.plane) {
+            for (int g = 0; g < TG::PLANE_ELEMS; ++g) {
+                long long vo;
+                int so;
+                twopass_plane_elem<TG>(it.j, g, &vo, &so);
+                sm[so] = in[it.vol * TG::V + vo];
+            }
+            for (int r = 0; r < G * N1; ++r) pass_z<XG, S, ALG_DEFAULT>(sm.data(), r);
+            for (int l = 0; l < G * N2; ++l) pass_y<XG, S, ALG_DEFAULT>(sm.data(), l);
+            for (int g = 0; g < TG::PLANE_ELEMS; ++g) {
+                long long vo;
+                int so;
+                twopass_plane_elem<TG>(it.j, g, &vo, &so);
+                sv[vo] = sm[so];
+            }
+        } else {
+            for (int g = 0; g < TG::ROW_ELEMS; ++g) {
+                long long vo;
+                int so;
+                twopass_row_elem<TG>(it.j, g, &vo, &so);
+                sm[so] = sv[vo];
+            }
+            for (int l = 0; l < G * N2; ++l)
+                pass_x_slab<YG, S, N1>(sm.data(), l, out + it.vol * TG::V, it.j * G, scale);
+        }
+    }
+}
+
 typedef void (*emu_fn)(const void *, void *, long long);
+
+#define EMU_TP(N0, N1, N2, T, G)                                                              \
+    {N0, N1, N2, sizeof(T) == 8 ? 0 : 1, -1, 300 + G, 1,                                    \
+     &emulate_twopass<N0, N1, N2, T, -1, G>},                                                \
+    {N0, N1, N2, sizeof(T) == 8 ? 0 : 1, +1, 300 + G, 1, &emulate_twopass<N0, N1, N2, T, +1, G>}
 
 #define EMU_BIG(L, T, PL)                                                               \
     {L, L, L, sizeof(T) == 8 ? 0 : 1, -1, 200 + PL, 1, &emulate_big_cube<L, T, -1, PL>}, \
@@ -148,6 +212,9 @@ static const EmuEntry kEmu[] = {
     EMU_CL(36, 36, 36, double, 4), EMU_CL(36, 36, 36, double, 6),  EMU_CL(36, 36, 36, double, 9),
     EMU_CL(36, 36, 36, float, 2),  EMU_CL(36, 36, 36, float, 4),   EMU_CL(36, 36, 36, float, 6),
     EMU_BIG(36, double, 9),        EMU_BIG(36, float, 12),
+    EMU_TP(36, 36, 36, double, 4), EMU_TP(36, 36, 36, double, 2),  EMU_TP(36, 36, 36, double, 6),
+    EMU_TP(36, 36, 36, float, 4),  EMU_TP(36, 36, 36, float, 6),   EMU_TP(16, 16, 32, double, 4),
+    EMU_TP(16, 16, 32, double, 8), EMU_TP(6, 9, 5, double, 3),
 };
 
 // The chain kernel's per-CTA loop (chain_kernels.cu k_chain) for one volume per CTA.
@@ -186,6 +253,15 @@ extern "C" int hostcheck_chain(int n, int prec, int epi, const void *in, void *o
     HC_CHAIN(6, double) HC_CHAIN(8, double) HC_CHAIN(17, double) HC_CHAIN(8, float)
 #undef HC_CHAIN
     return -2;
+}
+
+// Items whose dependency wait would not hold when taken in ticket order (the
+// TWOPASS deadlock-freedom argument); reset by reading.
+extern "C" long long hostcheck_twopass_violations()
+{
+    const long long v = g_twopass_violations;
+    g_twopass_violations = 0;
+    return v;
 }
 
 extern "C" int hostcheck_fft3d(int n0, int n1, int n2, int prec, int sign, int alg, int vpc,

@@ -47,14 +47,36 @@ const std::vector<KernelEntry> &registry()
         register_tc_kernels(reg);
         register_kernels(reg);
         register_cluster_kernels(reg);
+        register_twopass_kernels(reg);
     });
     return reg;
 }
 
 cudaError_t launch_entry(const KernelEntry &e, const void *in, void *out, long long nvol,
-                         double scale, cudaStream_t stream, int grid_limit, int *err)
+                         double scale, cudaStream_t stream, int grid_limit, int *err, void *work)
 {
     if (nvol <= 0) return cudaSuccess;
+    if (e.family == FAM_TWOPASS) {
+        if (!work) return cudaErrorInvalidValue;
+        const long long items = (long long)(e.n0 / e.vpc + e.n1 / e.vpc) * nvol;
+        const long long grid = std::max(1LL, std::min(items, (long long)grid_limit));
+        int lag = 0;
+        int ring = twopass_ring(e, grid, &lag);
+        unsigned char *w = (unsigned char *)work;
+        if (e.precision == FFT3D_B200_C128) {
+            double s = scale;
+            void *args[] = {(void *)&in, (void *)&out, (void *)&nvol, (void *)&s,
+                            (void *)&err, (void *)&w,  (void *)&ring, (void *)&lag};
+            return cudaLaunchKernel(e.func, dim3((unsigned)grid), dim3(e.threads), args,
+                                    (size_t)e.smem, stream);
+        } else {
+            float s = (float)scale;
+            void *args[] = {(void *)&in, (void *)&out, (void *)&nvol, (void *)&s,
+                            (void *)&err, (void *)&w,  (void *)&ring, (void *)&lag};
+            return cudaLaunchKernel(e.func, dim3((unsigned)grid), dim3(e.threads), args,
+                                    (size_t)e.smem, stream);
+        }
+    }
     if (e.family == FAM_STREAM) {
         const long long items = (nvol + e.vpc - 1) / e.vpc;
         const long long grid = std::max(1LL, std::min(items, (long long)grid_limit));
@@ -223,11 +245,20 @@ static const KernelEntry *tune(const std::vector<const KernelEntry *> &cands, in
         const int occ = entry_occupancy(*k, device);
         if (occ <= 0) continue;
         const int glim = occ * num_sms;
+        void *work = nullptr;
+        const size_t wb = entry_workspace_bytes(*k, glim);
+        if (wb && (cudaMalloc(&work, wb) != cudaSuccess ||
+                   cudaMemset(work, 0, TWOPASS_CTL_BYTES) != cudaSuccess)) {
+            cudaGetLastError();
+            if (work) cudaFree(work);
+            continue;
+        }
         bool ok = true;
         for (int w = 0; w < 2 && ok; ++w)
-            ok = launch_entry(*k, bufs[0], bufs[1], nb, 1.0, s, glim, err) == cudaSuccess;
+            ok = launch_entry(*k, bufs[0], bufs[1], nb, 1.0, s, glim, err, work) == cudaSuccess;
         if (!ok || cudaStreamSynchronize(s) != cudaSuccess) {
             cudaGetLastError();
+            if (work) cudaFree(work);
             continue;
         }
         float ms_min = 1e30f;
@@ -236,13 +267,17 @@ static const KernelEntry *tune(const std::vector<const KernelEntry *> &cands, in
             cudaEventRecord(e0, s);
             for (int it = 0; it < reps; ++it) {
                 const int j = it % nsets;
-                launch_entry(*k, bufs[2 * j], bufs[2 * j + 1], nb, 1.0, s, glim, err);
+                launch_entry(*k, bufs[2 * j], bufs[2 * j + 1], nb, 1.0, s, glim, err, work);
             }
             cudaEventRecord(e1, s);
             cudaEventSynchronize(e1);
             float ms = 0.f;
             cudaEventElapsedTime(&ms, e0, e1);
             ms_min = std::min(ms_min, ms / (float)reps);
+        }
+        if (work) {
+            cudaStreamSynchronize(s);
+            cudaFree(work);
         }
         if (log) {
             char buf[256];
@@ -264,19 +299,24 @@ static const KernelEntry *tune(const std::vector<const KernelEntry *> &cands, in
 const KernelEntry *tuned_entry(int device, int n0, int n1, int n2, int precision, int sign,
                                long long batch)
 {
-    auto cands = candidates(n0, n1, n2, precision, sign);
+    // kernels that need no workspace: the caller launches on several streams at once
+    std::vector<const KernelEntry *> cands;
+    for (const KernelEntry *k : candidates(n0, n1, n2, precision, sign))
+        if (k->family != FAM_TWOPASS) cands.push_back(k);
     if (cands.empty()) return nullptr;
+    // a memo of its own: plan creation may pick a workspace kernel for the same key
+    static std::map<std::tuple<int, int, int, int, int, int, int>, const KernelEntry *> memo;
     auto key = std::make_tuple(device, n0, n1, n2, precision, sign, batch_bucket(batch));
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    auto it = g_tuned.find(key);
-    if (it != g_tuned.end()) return it->second;
+    auto it = memo.find(key);
+    if (it != memo.end()) return it->second;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     const KernelEntry *k =
         getenv("FFT3D_B200_NO_TUNE")
             ? cands[0]
             : tune(cands, device, batch, precision, (long long)n0 * n1 * n2, sms, nullptr, nullptr);
-    g_tuned[key] = k;
+    memo[key] = k;
     return k;
 }
 
@@ -294,6 +334,10 @@ struct fft3d_b200_plan {
     const KernelEntry *kernel;
     int grid_limit;          // persistent families: CTAs per SM x SMs
     int *d_err = nullptr;    // device error word (bounded-wait timeouts)
+    // kernel workspace (TWOPASS scratch ring): [0] for device-pointer executes,
+    // [1] for the second stream of host-pointer executes; 0 bytes for other families
+    size_t work_bytes = 0;
+    void *work[2] = {nullptr, nullptr};
     std::string describe;
     // host-pointer execution
     void *d_in = nullptr, *d_out = nullptr;
@@ -327,6 +371,21 @@ extern "C" int fft3d_b200_variants(int n0, int n1, int n2, int precision, int di
     auto c = candidates(n0, n1, n2, precision, direction);
     for (int i = 0; i < (int)c.size() && i < max && names; ++i) names[i] = c[i]->name;
     return (int)c.size();
+}
+
+// Allocate workspace `i` of a plan whose kernel needs one; its control block
+// starts zeroed (each launch leaves it zeroed again).
+static int ensure_work(fft3d_b200_plan *p, int i)
+{
+    if (!p->work_bytes || p->work[i]) return FFT3D_B200_OK;
+    if (cudaMalloc(&p->work[i], p->work_bytes) != cudaSuccess ||
+        cudaMemset(p->work[i], 0, TWOPASS_CTL_BYTES) != cudaSuccess) {
+        cudaGetLastError();
+        if (p->work[i]) cudaFree(p->work[i]);
+        p->work[i] = nullptr;
+        return FFT3D_B200_ERR_NOMEM;
+    }
+    return FFT3D_B200_OK;
 }
 
 static int plan_create_impl(const fft3d_b200_desc *desc, const char *variant,
@@ -410,6 +469,13 @@ static int plan_create_impl(const fft3d_b200_desc *desc, const char *variant,
     p->kernel = k;
     p->grid_limit = entry_occupancy(*k, device) * sms;
     p->describe = k->name;
+    p->work_bytes = entry_workspace_bytes(*k, p->grid_limit);
+    if (p->work_bytes && ensure_work(p, 0) != FFT3D_B200_OK) {
+        cudaFree(p->d_err);
+        delete p;
+        if (prev >= 0) cudaSetDevice(prev);
+        return set_status(FFT3D_B200_ERR_NOMEM);
+    }
     if (prev >= 0 && prev != device) cudaSetDevice(prev);
     *out = p;
     return set_status(FFT3D_B200_OK);
@@ -477,6 +543,8 @@ extern "C" void fft3d_b200_plan_destroy(fft3d_b200_plan *p)
     cudaDeviceSynchronize();
     free_staging(p);
     if (p->d_err) cudaFree(p->d_err);
+    for (void *w : p->work)
+        if (w) cudaFree(w);
     if (prev >= 0) cudaSetDevice(prev);
     delete p;
 }
@@ -496,7 +564,7 @@ extern "C" int fft3d_b200_execute(fft3d_b200_plan *p, const void *d_in, void *d_
     if (((uintptr_t)d_in % al) || ((uintptr_t)d_out % al)) return set_status(FFT3D_B200_ERR_ALIGN);
     if (ranges_overlap(d_in, d_out, p->bytes)) return set_status(FFT3D_B200_ERR_OVERLAP);
     cudaError_t e = launch_entry(*p->kernel, d_in, d_out, p->desc.batch, p->scale,
-                                 (cudaStream_t)stream, p->grid_limit, p->d_err);
+                                 (cudaStream_t)stream, p->grid_limit, p->d_err, p->work[0]);
     if (e != cudaSuccess) return set_status(FFT3D_B200_ERR_CUDA);
     return set_status(FFT3D_B200_OK);
 }
@@ -572,6 +640,9 @@ static int run_host_chain(fft3d_b200_plan *const *plans, int nplans, const void 
     fft3d_b200_plan *p = plans[0];
     int st = ensure_staging(p);
     if (st) return st;
+    // chunks alternate over two streams: a second workspace for the second one
+    for (int i = 0; i < nplans; ++i)
+        if ((st = ensure_work(plans[i], 1)) != FFT3D_B200_OK) return st;
     const size_t eb = (size_t)element_bytes(p->desc.precision);
     const size_t vb = (size_t)p->vol_elems * eb;
     const bool pinned = is_pinned(h_in) && is_pinned(h_out);
@@ -605,7 +676,7 @@ static int run_host_chain(fft3d_b200_plan *const *plans, int nplans, const void 
         char *a = din, *b = dout;
         for (int i = 0; i < nplans; ++i) {
             err = launch_entry(*plans[i]->kernel, a, b, nv, plans[i]->scale, s,
-                               plans[i]->grid_limit, plans[i]->d_err);
+                               plans[i]->grid_limit, plans[i]->d_err, plans[i]->work[slot]);
             if (err != cudaSuccess) return FFT3D_B200_ERR_CUDA;
             std::swap(a, b);
         }

@@ -16,8 +16,50 @@ constexpr int DEV_ERR_NONE = 0;
 constexpr int DEV_ERR_LOAD_TIMEOUT = 1;    // a stage load never completed
 constexpr int DEV_ERR_CLUSTER_TIMEOUT = 2; // a cluster peer never arrived
 constexpr int DEV_ERR_QUEUE_TIMEOUT = 3;   // a work-queue flag never became ready
+constexpr int DEV_ERR_DEP_TIMEOUT = 4;     // a two-pass dependency counter never arrived
 
 constexpr uint32_t kSpinLimit = 1u << 24;
+// Wall-clock bound of a wait on a global counter that other CTAs advance.
+constexpr unsigned long long kCounterWaitNs = 2000000000ull;  // 2 s
+
+__device__ __forceinline__ unsigned long long globaltimer_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Load with acquire semantics at GPU scope.
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Add with release semantics at GPU scope (no return value).
+__device__ __forceinline__ void red_release_gpu_add(unsigned *p, unsigned v)
+{
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Wait until *p >= target, or *abort becomes nonzero, or kCounterWaitNs pass.
+// Returns true when the target was reached.  One thread calls it.
+__device__ __forceinline__ bool wait_counter_geq(const unsigned *p, unsigned target,
+                                                 const unsigned *abort)
+{
+    if (ld_acquire_gpu(p) >= target) return true;
+    const unsigned long long t0 = globaltimer_ns();
+    unsigned ns = 32;
+    for (uint32_t i = 0; i < kSpinLimit; ++i) {
+        __nanosleep(ns);
+        if (ns < 1024) ns *= 2;
+        if (ld_acquire_gpu(p) >= target) return true;
+        if (ld_acquire_gpu(abort) != 0) return false;
+        if (globaltimer_ns() - t0 > kCounterWaitNs) return false;
+    }
+    return false;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
 {

@@ -76,6 +76,9 @@ def test_every_variant_matches_oracle(shape, prec, direction):
             # persistent kernels: every CTA walks >= 2 groups and one group is partial
             vpc = int(v.split(" vpc")[1].split()[0])
             b = 2 * 148 * vpc + vpc // 2 + 1
+        elif v.startswith("twopass"):
+            # beyond the scratch ring (about 40 volumes at a full grid): slots are reused
+            b = 100
         x = field(rng, (b,) + shape, dtype=NDT[prec])
         want = ref(x, direction)
         plan = fb.Plan(shape, b, direction, prec, variant=v)

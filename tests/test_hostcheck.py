@@ -97,6 +97,33 @@ def test_two_phase_cube(hostcheck, prec, pl, sign):
     assert err < (C128_TOL if prec == 0 else C64_TOL), err
 
 
+TWOPASS = [((36, 36, 36), 0, 4, 11), ((36, 36, 36), 0, 2, 3), ((36, 36, 36), 0, 6, 9),
+           ((36, 36, 36), 1, 4, 11), ((36, 36, 36), 1, 6, 2), ((16, 16, 32), 0, 4, 13),
+           ((16, 16, 32), 0, 8, 1), ((6, 9, 5), 0, 3, 41)]
+
+
+@pytest.mark.parametrize("shape,prec,g,nvol", TWOPASS,
+                         ids=[f"{t[0]}-c{128 if t[1] == 0 else 64}-g{t[2]}-b{t[3]}" for t in TWOPASS])
+@pytest.mark.parametrize("sign", [-1, +1])
+def test_twopass_items(hostcheck, shape, prec, g, nvol, sign):
+    """The TWOPASS kernel's plane and row items in ticket order (alg = 300 + G):
+    decode, element maps, scratch-ring reuse; batches below and above the lag D
+    and the ring size R.  Every dependency wait must already hold in ticket
+    order -- the property that makes the kernel's order deadlock-free."""
+    import ctypes
+    hostcheck.hostcheck_twopass_violations.restype = ctypes.c_longlong
+    hostcheck.hostcheck_twopass_violations()
+    rng = np.random.default_rng(5000 + g + nvol + prec)
+    dt = np.complex128 if prec == 0 else np.complex64
+    x = field(rng, (nvol,) + shape, dist="normal", dtype=dt)
+    got = run(hostcheck, x, shape, prec, sign, 300 + g, 1)
+    assert hostcheck.hostcheck_twopass_violations() == 0
+    x64 = x.astype(np.complex128)
+    want = oracle.fft3d(x64) if sign < 0 else oracle.ifft3d(x64)
+    err = oracle.rel_error_per_volume(got, want).max()
+    assert err < (C128_TOL if prec == 0 else C64_TOL), err
+
+
 GOLD = [p for p in sorted(glob.glob(os.path.join(GOLDEN, "vol_*.npz")))]
 
 

@@ -213,6 +213,15 @@ void register_twopass_kernels(std::vector<KernelEntry> &out)
     // 16x16x32 complex double (262 KB): z pass 16*G rows, y and x passes 32*G lines
     FFT3D_TWOPASS(16, 16, 32, double, 4, 128, 4);
     FFT3D_TWOPASS(16, 16, 32, double, 8, 256, 2);
+    // 45^3 (45 = 5 x 9) and 64^3 (64 = 8 x 8): beyond any cluster's shared memory
+    FFT3D_TWOPASS(45, 45, 45, double, 3, 160, 2);
+    FFT3D_TWOPASS(45, 45, 45, double, 5, 256, 1);
+    FFT3D_TWOPASS(45, 45, 45, float, 5, 256, 2);
+    FFT3D_TWOPASS(45, 45, 45, float, 3, 160, 3);
+    FFT3D_TWOPASS(64, 64, 64, double, 1, 64, 3);
+    FFT3D_TWOPASS(64, 64, 64, double, 2, 128, 1);
+    FFT3D_TWOPASS(64, 64, 64, float, 2, 128, 3);
+    FFT3D_TWOPASS(64, 64, 64, float, 4, 256, 1);
 }
 
 }  // namespace fft3d

@@ -78,6 +78,8 @@ void register_kernels(std::vector<KernelEntry> &out)
     FFT3D_VOL(24, 24, 24, double, 0, 1, 288, 1);
     FFT3D_VOL(8, 8, 16, double, 0, 8, 512, 1);
     FFT3D_VOL(16, 16, 32, double, 0, 1, 256, 1);
+    FFT3D_VOL(13, 13, 13, double, 0, 2, 352, 1);
+    FFT3D_VOL(23, 23, 23, double, 0, 1, 288, 1);
     // complex float
     FFT3D_VOL(6, 6, 6, float, 0, 32, 512, 1);
     FFT3D_VOL(8, 8, 8, float, 0, 16, 512, 1);
@@ -87,6 +89,8 @@ void register_kernels(std::vector<KernelEntry> &out)
     FFT3D_VOL(24, 24, 24, float, 0, 1, 576, 1);
     FFT3D_VOL(8, 8, 16, float, 0, 16, 1024, 1);
     FFT3D_VOL(16, 16, 32, float, 0, 1, 512, 1);
+    FFT3D_VOL(13, 13, 13, float, 0, 4, 704, 1);
+    FFT3D_VOL(23, 23, 23, float, 0, 1, 544, 1);
 }
 
 }  // namespace fft3d

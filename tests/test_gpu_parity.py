@@ -29,7 +29,8 @@ C128_TOL = 1e-13
 C64_TOL = 2e-6
 
 GEOMS = [(6, 6, 6), (8, 8, 8), (12, 12, 12), (16, 16, 16), (17, 17, 17), (24, 24, 24),
-         (8, 8, 16), (16, 16, 32), (36, 36, 36)]
+         (8, 8, 16), (16, 16, 32), (36, 36, 36), (13, 13, 13), (23, 23, 23), (45, 45, 45),
+         (64, 64, 64)]
 TDT = {fb.C128: torch.complex128, fb.C64: torch.complex64}
 NDT = {fb.C128: np.complex128, fb.C64: np.complex64}
 
@@ -71,6 +72,8 @@ def test_every_variant_matches_oracle(shape, prec, direction):
     rng = np.random.default_rng(abs(hash((shape, prec, direction))) % 2**31)
     tol = C128_TOL if prec == fb.C128 else C64_TOL
     for v in fb.variants(shape, prec, direction):
+        # the two-term split-BF16 tensor-core variant keeps 16 bits (bound of test_gpu_tensor.py)
+        tol = 3e-5 if "split2" in v else (C128_TOL if prec == fb.C128 else C64_TOL)
         b = batch_for(shape, prec)
         if v.startswith("stream"):
             # persistent kernels: every CTA walks >= 2 groups and one group is partial

@@ -24,10 +24,11 @@ GEOMS = [((6, 6, 6), 0, 16), ((8, 8, 8), 0, 8), ((12, 12, 12), 0, 2), ((16, 16, 
          ((16, 16, 32), 0, 1), ((36, 36, 36), 0, 1), ((2, 3, 5), 0, 3), ((7, 11, 13), 0, 2),
          ((9, 9, 9), 0, 2), ((5, 8, 12), 0, 1), ((32, 8, 4), 0, 1), ((13, 5, 8), 0, 1),
          ((4, 4, 4), 0, 2), ((1, 8, 8), 0, 1), ((8, 1, 8), 0, 1), ((8, 8, 1), 0, 1),
-         ((1, 1, 1), 0, 1), ((3, 3, 3), 0, 1), ((17, 2, 2), 0, 1)]
+         ((1, 1, 1), 0, 1), ((3, 3, 3), 0, 1), ((17, 2, 2), 0, 1), ((13, 13, 13), 0, 2),
+         ((23, 23, 23), 0, 1)]
 GEOMS64 = [((6, 6, 6), 0, 32), ((8, 8, 8), 0, 16), ((12, 12, 12), 0, 4), ((16, 16, 16), 0, 2),
            ((17, 17, 17), 0, 2), ((17, 17, 17), 1, 2), ((24, 24, 24), 0, 1), ((8, 8, 16), 0, 16),
-           ((16, 16, 32), 0, 1), ((36, 36, 36), 0, 1)]
+           ((16, 16, 32), 0, 1), ((36, 36, 36), 0, 1), ((13, 13, 13), 0, 4), ((23, 23, 23), 0, 1)]
 
 
 def run(hc, x, shape, prec, sign, alg, vpc):
@@ -99,7 +100,8 @@ def test_two_phase_cube(hostcheck, prec, pl, sign):
 
 TWOPASS = [((36, 36, 36), 0, 4, 11), ((36, 36, 36), 0, 2, 3), ((36, 36, 36), 0, 6, 9),
            ((36, 36, 36), 1, 4, 11), ((36, 36, 36), 1, 6, 2), ((16, 16, 32), 0, 4, 13),
-           ((16, 16, 32), 0, 8, 1), ((6, 9, 5), 0, 3, 41)]
+           ((16, 16, 32), 0, 8, 1), ((6, 9, 5), 0, 3, 41), ((45, 45, 45), 0, 3, 5),
+           ((45, 45, 45), 1, 5, 3), ((64, 64, 64), 0, 1, 3), ((64, 64, 64), 1, 2, 2)]
 
 
 @pytest.mark.parametrize("shape,prec,g,nvol", TWOPASS,

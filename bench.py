@@ -37,6 +37,9 @@ sys.path.insert(0, os.path.join(ROOT, "opt-fft_b200"))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 L2_BYTES = 126 * 1024 * 1024
+# how the device-timed region was launched (filled in by time_device)
+TIMING = {"launch": "timed steps captured in one CUDA graph, replayed once between two events; "
+                    "per-launch times from event record nodes", "graph_uploaded": None}
 
 WORKLOADS = {
     "roundtrip17": dict(shape=(17, 17, 17), batch=2048, prec=0, chain=(-1, +1), dist="uniform",
@@ -197,27 +200,79 @@ class Workload:
         return sum(p.launches() for p in self.plans)
 
 
+class CopyFloor:
+    """A device-to-device copy of the same bytes as the first launch of a
+    workload's step, over the same rotating buffers: what the memory system
+    delivers at this transfer size (small transfers do not reach the
+    large-buffer copy peak)."""
+
+    def __init__(self, wl):
+        self.wl = wl
+        self.it = 0
+
+    def step(self, stream, ev=None):
+        bufs = self.wl.sets[self.it % self.wl.nsets]
+        self.it += 1
+        if ev is not None:
+            ev[0].record(stream)
+        bufs[1].copy_(bufs[0])
+        if ev is not None:
+            ev[1].record(stream)
+
+
+def copy_floor(torch, wl, stream, steps, warmup):
+    """GB/s (read + write) of a same-size device copy, timed like the kernel."""
+    with torch.cuda.stream(stream):
+        _, per_ms, _ = time_device(torch, CopyFloor(wl), stream, steps, warmup)
+    return 2 * wl.bytes / (per_ms * 1e-3) / 1e9
+
+
+def _graph_upload(torch, graph, stream):
+    """cudaGraphUpload of a captured graph, so that its first replay is not
+    charged for moving the executable graph to the device."""
+    path = next((ln.split()[-1] for ln in open("/proc/self/maps") if "libcudart.so" in ln), None)
+    if path is None:
+        return False
+    rt = ctypes.CDLL(path)
+    rt.cudaGraphUpload.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    return rt.cudaGraphUpload(ctypes.c_void_p(graph.raw_cuda_graph_exec()),
+                              ctypes.c_void_p(stream.cuda_stream)) == 0
+
+
 def time_device(torch, wl, stream, steps, warmup, dist=None, sampler=None):
+    """Device time of `steps` steps: W eager warm-up steps, then the K timed
+    steps captured into one CUDA graph (the launch path a serving loop uses),
+    uploaded, and replayed once between two events.  Without the graph a
+    kernel of ~15 us waits on the Python loop that enqueues it, and that host
+    time would be charged to the kernel.  Per-launch durations come from event
+    record nodes around the first launch of every step."""
     for _ in range(warmup):
         wl.step(stream)
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True, external=True),
+            torch.cuda.Event(enable_timing=True, external=True)) for _ in range(steps)]
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=stream):
+        for k in range(steps):
+            wl.step(stream, evs[k])
+    uploaded = _graph_upload(torch, graph, stream)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
     if sampler:
         sampler.start()
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(steps)]
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record(stream)
-    for k in range(steps):
-        wl.step(stream, evs[k])
-    e1.record(stream)
+    with torch.cuda.stream(stream):  # replay() launches on the current stream
+        e0.record(stream)
+        graph.replay()
+        e1.record(stream)
     torch.cuda.synchronize()
     clocks = sampler.stop() if sampler else None
+    TIMING["graph_uploaded"] = uploaded
     total_ms = e0.elapsed_time(e1)
     first_ms = [a.elapsed_time(b) for a, b in evs]
+    del graph
     if dist is not None:
         t = torch.tensor([total_ms], dtype=torch.float64, device=stream.device)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -602,6 +657,9 @@ def main():
                 "alg_bytes_per_launch": alg_bytes,
                 "traffic": traffic.get(a.workload.replace("roundtrip", "fwd")),
                 "ms_per_launch": first_ms}
+    cf = copy_floor(torch, wl, stream, min(a.steps, 200), a.warmup)
+    roofline["copy_same_bytes_gbs"] = cf
+    roofline["frac_of_copy_same_bytes"] = achieved / cf
 
     e2e = None
     if not a.no_e2e:
@@ -625,8 +683,10 @@ def main():
             m, f, _ = time_device(torch, x, stream, max(5, a.steps // 2), a.warmup, dist, None)
             ab = 2 * x.bytes
             ach = ab / (f * 1e-3) / 1e9
+            cfx = copy_floor(torch, x, stream, max(5, a.steps // 2), a.warmup)
             workloads[name] = {"label": ww["label"], "volumes_per_s": world * x.batch / (m * 1e-3),
                                "ms_per_launch": f, "achieved_gbs": ach, "frac": ach / peak,
+                               "copy_same_bytes_gbs": cfx, "frac_of_copy_same_bytes": ach / cfx,
                                "kernel": x.plans[0].describe(),
                                "traffic": traffic.get(name)}
             del x
@@ -657,7 +717,8 @@ def main():
                        "step": "forward+inverse" if len(w["chain"]) == 2 else "forward",
                        "l2": (f"inputs larger than L2 ({wl.bytes / 2**20:.0f} MiB per buffer, "
                               f"{wl.nsets} rotating buffer sets)"),
-                       "parallelism": f"dp{world} (volumes sharded, no collective)"},
+                       "parallelism": f"dp{world} (volumes sharded, no collective)",
+                       "timing": dict(TIMING)},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "clocks": clocks, "gpu_launches": a.steps * wl.launches_per_step(),
             "workloads": workloads}

@@ -111,6 +111,29 @@ int fft3d_b200_last_status(void);
 
 const char *fft3d_b200_status_string(int status);
 
+/* ---------------------------------------------------------------- plan wisdom
+ *
+ * The autotuner's choices -- device type (name, compute capability, SM count),
+ * extents, precision, direction and batch-size class -> kernel variant -- kept
+ * per process and saved to / loaded from a text file, so that later processes
+ * on the same kind of GPU skip the plan-time timing race.  Replaces the
+ * reference's per-create race (bench/geom/best/fft3d_best.c:148-193) by the
+ * persisted per-host form bench/gen/PANEL_BRIEF.md:12-20 asks for; no
+ * counterpart function exists in the reference.
+ *
+ * With FFT3D_B200_WISDOM=<path> set, the file is read at the first plan
+ * creation and rewritten after each new choice.  Entries for device types not
+ * present are kept; entries naming variants this build lacks are ignored. */
+
+/* Write the choices made or imported so far; entries written, or an error code. */
+int fft3d_b200_wisdom_export(const char *path);
+
+/* Merge a wisdom file into this process's choices; entries taken, or an error code. */
+int fft3d_b200_wisdom_import(const char *path);
+
+/* Drop every remembered choice (plans created afterwards time their candidates again). */
+void fft3d_b200_wisdom_forget(void);
+
 /* ---------------------------------------------------------------- batches of uneven geometry */
 
 typedef struct {

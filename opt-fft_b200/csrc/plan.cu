@@ -373,6 +373,145 @@ extern "C" int fft3d_b200_variants(int n0, int n1, int n2, int precision, int di
     return (int)c.size();
 }
 
+// ------------------------------------------------------------------ wisdom
+//
+// The plan-time race (bench/geom/best/fft3d_best.c:148-193) generalised to a
+// per-host cache (bench/gen/PANEL_BRIEF.md:12-20): the tuner's choices are
+// written as text, one per line,
+//     <device name>|sm<major>.<minor>|<SMs> TAB <n0 n1 n2 precision sign bucket> TAB <variant>
+// and read back into the memo for every visible device of the same type, so a
+// later process skips the timing.  Lines for device types not present here are
+// kept and written back unchanged.  The memo mutex (g_tune_mu) guards all of it.
+
+namespace fft3d {
+
+static std::vector<std::string> g_wisdom_foreign;
+static bool g_wisdom_autoloaded = false;
+
+static std::string device_tag(int device)
+{
+    cudaDeviceProp pr;
+    if (cudaGetDeviceProperties(&pr, device) != cudaSuccess) {
+        cudaGetLastError();
+        return std::string();
+    }
+    char buf[400];
+    snprintf(buf, sizeof buf, "%s|sm%d.%d|%d", pr.name, pr.major, pr.minor, pr.multiProcessorCount);
+    for (char *c = buf; *c; ++c)
+        if (*c == '\t' || *c == '\n') *c = ' ';
+    return buf;
+}
+
+// Write the memo (and the kept foreign lines) to `path` via a temporary file.
+static int wisdom_write(const char *path)
+{
+    const std::string tmp = std::string(path) + ".tmp";
+    FILE *f = fopen(tmp.c_str(), "w");
+    if (!f) return FFT3D_B200_ERR_INVALID;
+    fprintf(f, "fft3d_b200 wisdom 1\n");
+    int n = 0;
+    std::map<int, std::string> tags;
+    for (const auto &kv : g_tuned) {
+        int dev, n0, n1, n2, prec, sign, bucket;
+        std::tie(dev, n0, n1, n2, prec, sign, bucket) = kv.first;
+        if (!tags.count(dev)) tags[dev] = device_tag(dev);
+        if (tags[dev].empty() || !kv.second) continue;
+        fprintf(f, "%s\t%d %d %d %d %d %d\t%s\n", tags[dev].c_str(), n0, n1, n2, prec, sign, bucket,
+                kv.second->name);
+        ++n;
+    }
+    for (const auto &line : g_wisdom_foreign) fprintf(f, "%s\n", line.c_str());
+    const bool ok = fclose(f) == 0;
+    if (!ok || rename(tmp.c_str(), path) != 0) {
+        remove(tmp.c_str());
+        return FFT3D_B200_ERR_INVALID;
+    }
+    return n;
+}
+
+// Merge the entries of `path` into the memo; returns entries taken or an error.
+static int wisdom_read(const char *path)
+{
+    FILE *f = fopen(path, "r");
+    if (!f) return FFT3D_B200_ERR_INVALID;
+    char line[1024];
+    if (!fgets(line, sizeof line, f) || strncmp(line, "fft3d_b200 wisdom 1", 19) != 0) {
+        fclose(f);
+        return FFT3D_B200_ERR_INVALID;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess) {
+        cudaGetLastError();
+        ndev = 0;
+    }
+    std::vector<std::string> tags(ndev);
+    for (int d = 0; d < ndev; ++d) tags[d] = device_tag(d);
+    int taken = 0;
+    while (fgets(line, sizeof line, f)) {
+        std::string s(line);
+        while (!s.empty() && (s.back() == '\n' || s.back() == '\r')) s.pop_back();
+        const size_t t1 = s.find('\t'), t2 = t1 == std::string::npos ? t1 : s.find('\t', t1 + 1);
+        if (t2 == std::string::npos) continue;  // malformed: ignored
+        const std::string tag = s.substr(0, t1), name = s.substr(t2 + 1);
+        int n0, n1, n2, prec, sign, bucket;
+        if (sscanf(s.c_str() + t1 + 1, "%d %d %d %d %d %d", &n0, &n1, &n2, &prec, &sign, &bucket) != 6)
+            continue;
+        const KernelEntry *e = nullptr;
+        for (const auto &r : registry())
+            if (name == r.name && r.n0 == n0 && r.n1 == n1 && r.n2 == n2 && r.precision == prec &&
+                r.sign == sign)
+                e = &r;
+        bool matched = false;
+        for (int d = 0; d < ndev; ++d) {
+            if (tags[d].empty() || tags[d] != tag) continue;
+            matched = true;
+            if (!e) continue;  // a variant this build does not have
+            g_tuned[std::make_tuple(d, n0, n1, n2, prec, sign, bucket)] = e;
+            ++taken;
+        }
+        if (!matched && std::find(g_wisdom_foreign.begin(), g_wisdom_foreign.end(), s) ==
+                            g_wisdom_foreign.end())
+            g_wisdom_foreign.push_back(s);
+    }
+    fclose(f);
+    return taken;
+}
+
+// FFT3D_B200_WISDOM=<path>: read once, at the first plan creation that tunes.
+static void wisdom_autoload()
+{
+    if (g_wisdom_autoloaded) return;
+    g_wisdom_autoloaded = true;
+    if (const char *w = getenv("FFT3D_B200_WISDOM")) wisdom_read(w);
+}
+
+}  // namespace fft3d
+
+extern "C" int fft3d_b200_wisdom_export(const char *path)
+{
+    if (!path) return fft3d::set_status(FFT3D_B200_ERR_INVALID);
+    std::lock_guard<std::mutex> lk(fft3d::g_tune_mu);
+    const int n = fft3d::wisdom_write(path);
+    fft3d::set_status(n < 0 ? n : FFT3D_B200_OK);
+    return n;
+}
+
+extern "C" int fft3d_b200_wisdom_import(const char *path)
+{
+    if (!path) return fft3d::set_status(FFT3D_B200_ERR_INVALID);
+    std::lock_guard<std::mutex> lk(fft3d::g_tune_mu);
+    const int n = fft3d::wisdom_read(path);
+    fft3d::set_status(n < 0 ? n : FFT3D_B200_OK);
+    return n;
+}
+
+extern "C" void fft3d_b200_wisdom_forget(void)
+{
+    std::lock_guard<std::mutex> lk(fft3d::g_tune_mu);
+    fft3d::g_tuned.clear();
+    fft3d::g_wisdom_foreign.clear();
+}
+
 // Allocate workspace `i` of a plan whose kernel needs one; its control block
 // starts zeroed (each launch leaves it zeroed again).
 static int ensure_work(fft3d_b200_plan *p, int i)
@@ -448,6 +587,7 @@ static int plan_create_impl(const fft3d_b200_desc *desc, const char *variant,
         auto key = std::make_tuple(device, desc->n0, desc->n1, desc->n2, desc->precision,
                                    desc->direction, batch_bucket(desc->batch));
         std::lock_guard<std::mutex> lk(g_tune_mu);
+        wisdom_autoload();
         auto it = g_tuned.find(key);
         if (it != g_tuned.end()) {
             k = it->second;
@@ -457,6 +597,7 @@ static int plan_create_impl(const fft3d_b200_desc *desc, const char *variant,
                      &log);
             g_tuned[key] = k;
             if (getenv("FFT3D_B200_TUNE_LOG")) fprintf(stderr, "fft3d_b200 tune: %s\n", log.c_str());
+            if (const char *w = getenv("FFT3D_B200_WISDOM")) wisdom_write(w);
         }
     }
     if (!k) k = cands[0];

@@ -80,13 +80,18 @@ EXPORTS = {
                     "fft3d_execute", "fft3d_destroy"],
     "fft3d_gpu_api.h": ["fft3d_gpu_name", "fft3d_gpu_description", "fft3d_gpu_supports",
                         "fft3d_gpu_create", "fft3d_gpu_execute", "fft3d_gpu_destroy"],
+    "fft3d_mgpu_api.h": ["fft3d_mgpu_name", "fft3d_mgpu_description", "fft3d_mgpu_supports",
+                         "fft3d_mgpu_create", "fft3d_mgpu_create_ex", "fft3d_mgpu_upload",
+                         "fft3d_mgpu_execute", "fft3d_mgpu_download", "fft3d_mgpu_destroy"],
     "fft3d_b200.h": ["fft3d_b200_supports", "fft3d_b200_plan_create", "fft3d_b200_plan_destroy",
                      "fft3d_b200_variants", "fft3d_b200_plan_create_variant",
                      "fft3d_b200_execute", "fft3d_b200_execute_host",
                      "fft3d_b200_execute_host_chain", "fft3d_b200_plan_describe",
                      "fft3d_b200_plan_check",
                      "fft3d_b200_plan_launches", "fft3d_b200_last_status",
-                     "fft3d_b200_status_string", "fft3d_b200_batch_create",
+                     "fft3d_b200_status_string", "fft3d_b200_wisdom_export",
+                     "fft3d_b200_wisdom_import", "fft3d_b200_wisdom_forget",
+                     "fft3d_b200_batch_create",
                      "fft3d_b200_batch_execute", "fft3d_b200_batch_destroy",
                      "fft3d_b200_batch_describe", "fft3d_b200_batch_execute_noalloc",
                      "fft3d_b200_chain_create", "fft3d_b200_chain_run",
@@ -117,6 +122,15 @@ def _load():
         "fft3d_gpu_create": ([i, i], vp),
         "fft3d_gpu_execute": ([vp, vp, vp], None),
         "fft3d_gpu_destroy": ([vp], None),
+        "fft3d_mgpu_name": ([], ctypes.c_char_p),
+        "fft3d_mgpu_description": ([], ctypes.c_char_p),
+        "fft3d_mgpu_supports": ([i, i], i),
+        "fft3d_mgpu_create": ([i, i, i, ctypes.POINTER(i)], vp),
+        "fft3d_mgpu_create_ex": ([i, i, i, ctypes.POINTER(i), i], vp),
+        "fft3d_mgpu_upload": ([vp, vp], None),
+        "fft3d_mgpu_execute": ([vp], None),
+        "fft3d_mgpu_download": ([vp, vp], None),
+        "fft3d_mgpu_destroy": ([vp], None),
         "fft3d_b200_supports": ([i, i, i, i], i),
         "fft3d_b200_plan_create": ([ctypes.POINTER(Desc), ctypes.POINTER(vp)], i),
         "fft3d_b200_plan_destroy": ([vp], None),
@@ -131,6 +145,9 @@ def _load():
         "fft3d_b200_plan_launches": ([vp], i),
         "fft3d_b200_last_status": ([], i),
         "fft3d_b200_status_string": ([i], ctypes.c_char_p),
+        "fft3d_b200_wisdom_export": ([ctypes.c_char_p], i),
+        "fft3d_b200_wisdom_import": ([ctypes.c_char_p], i),
+        "fft3d_b200_wisdom_forget": ([], None),
         "fft3d_b200_batch_create": ([ctypes.POINTER(Segment), i, ctypes.c_uint, i,
                                      ctypes.POINTER(vp)], i),
         "fft3d_b200_batch_execute": ([vp, vp], i),
@@ -179,6 +196,67 @@ def variants(shape, precision=C128, direction=FORWARD):
     arr = (ctypes.c_char_p * max(n, 1))()
     _lib.fft3d_b200_variants(n0, n1, n2, precision, direction, arr, n)
     return [arr[k].decode() for k in range(n)]
+
+
+def wisdom_export(path) -> int:
+    """Write the autotuner's choices to `path`; returns the entries written."""
+    n = _lib.fft3d_b200_wisdom_export(os.fsencode(path))
+    if n < 0:
+        raise Fft3dError(n, "wisdom_export")
+    return n
+
+
+def wisdom_import(path) -> int:
+    """Merge a wisdom file into this process's choices; returns the entries taken."""
+    n = _lib.fft3d_b200_wisdom_import(os.fsencode(path))
+    if n < 0:
+        raise Fft3dError(n, "wisdom_import")
+    return n
+
+
+def wisdom_forget():
+    """Forget every autotuner choice of this process."""
+    _lib.fft3d_b200_wisdom_forget()
+
+
+class MgpuPlan:
+    """One batch of L^3 complex128 cubes split over several GPUs of this process
+    (include/fft3d_mgpu_api.h): x-slabs in, the all-to-all fused into the first
+    kernel as peer stores, x pass on y-slabs.  `devices` may repeat a device."""
+
+    def __init__(self, L: int, batch: int, devices, inverse: bool = False):
+        self.L, self.batch, self.devices = L, batch, list(devices)
+        arr = (ctypes.c_int * len(self.devices))(*self.devices)
+        self._h = _lib.fft3d_mgpu_create_ex(L, batch, len(self.devices), arr, 1 if inverse else 0)
+        if not self._h:
+            raise Fft3dError(ERR_UNSUPPORTED, f"mgpu create L={L} batch={batch} devices={self.devices}")
+
+    def upload(self, x):
+        import numpy as np
+        x = np.ascontiguousarray(x, dtype=np.complex128)
+        if x.shape != (self.batch, self.L, self.L, self.L):
+            raise ValueError(f"expected {(self.batch, self.L, self.L, self.L)}, got {x.shape}")
+        _lib.fft3d_mgpu_upload(self._h, x.ctypes.data)
+
+    def execute(self):
+        _lib.fft3d_mgpu_execute(self._h)
+
+    def download(self):
+        import numpy as np
+        out = np.empty((self.batch, self.L, self.L, self.L), dtype=np.complex128)
+        _lib.fft3d_mgpu_download(self._h, out.ctypes.data)
+        return out
+
+    def close(self):
+        if self._h:
+            _lib.fft3d_mgpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _check(status, what):

@@ -11,6 +11,7 @@
 
 #include <vector>
 
+#include "mgpu.cuh"
 #include "twopass.cuh"
 #include "volume.cuh"
 
@@ -255,6 +256,79 @@ extern "C" int hostcheck_chain(int n, int prec, int epi, const void *in, void *o
     }
     HC_CHAIN(6, double) HC_CHAIN(8, double) HC_CHAIN(17, double) HC_CHAIN(8, float)
 #undef HC_CHAIN
+    return -2;
+}
+
+// The multi-GPU slab path (mgpu.cu): n "GPUs" as separate buffers, the same layout
+// functions, the z and y passes of each x-plane with each point stored into the
+// middle buffer of its y owner, then the x lines of each y-slab, then the
+// gather of download().  Poisoned middle buffers show any point not delivered.
+template <int L, int SGN>
+static void emulate_mgpu(int n, const cx<double> *in, cx<double> *out, long long B)
+{
+    using PG = Geom<1, L, L, double>;
+    using RG = Geom<L, 1, L, double>;
+    const MgpuShape m{L, n, L / n};
+    const size_t slab = (size_t)B * m.S * L * L;
+    std::vector<std::vector<cx<double>>> mid(n, std::vector<cx<double>>(slab, cx<double>{-1e300, 1e300}));
+    std::vector<std::vector<cx<double>>> res(n, std::vector<cx<double>>(slab));
+    std::vector<cx<double>> sm((size_t)PG::PV);
+    const double scale = SGN > 0 ? 1.0 / ((double)L * L * L) : 1.0;
+    for (int g = 0; g < n; ++g) {
+        for (long long p = 0; p < B * m.S; ++p) {
+            const long long b = p / m.S, x = g * m.S + p % m.S;
+            const cx<double> *src = in + (b * L + x) * (long long)L * L;  // upload(): x-slab g
+            for (int e = 0; e < L * L; ++e) sm[PG::off(e / L, e % L)] = src[e];
+            for (int r = 0; r < L; ++r) pass_z<PG, SGN, ALG_DEFAULT>(sm.data(), r);
+            for (int l = 0; l < L; ++l) pass_y<PG, SGN, ALG_DEFAULT>(sm.data(), l);
+            for (int e = 0; e < L * L; ++e) {
+                int h;
+                const long long off = mgpu_mid_offset(m, g, p, e / L, e % L, &h);
+                mid[h][off] = sm[PG::off(e / L, e % L)];
+            }
+        }
+    }
+    std::vector<cx<double>> row((size_t)RG::PV);
+    for (int h = 0; h < n; ++h) {
+        for (long long r = 0; r < B * m.S; ++r) {
+            const long long b = r / m.S;
+            const int yl = (int)(r % m.S);
+            for (int e = 0; e < L * L; ++e)
+                row[RG::off(e / L, e % L)] = mid[h][mgpu_yslab_offset(m, b, e / L, yl, e % L)];
+            for (int z = 0; z < L; ++z) {
+                cx<double> v[L];
+                for (int j = 0; j < L; ++j) v[j] = row[RG::off(j, z)];
+                dft<L, SGN, double>(v);
+                for (int j = 0; j < L; ++j) {
+                    cx<double> o = v[j];
+                    if (SGN > 0) o = cscale(o, scale);
+                    res[h][mgpu_yslab_offset(m, b, j, yl, z)] = o;
+                }
+            }
+        }
+    }
+    for (long long b = 0; b < B; ++b)  // download(): ky = h*S + yl
+        for (int kx = 0; kx < L; ++kx)
+            for (int ky = 0; ky < L; ++ky)
+                for (int kz = 0; kz < L; ++kz)
+                    out[((b * L + kx) * L + ky) * (long long)L + kz] =
+                        res[ky / m.S][mgpu_yslab_offset(m, b, kx, ky % m.S, kz)];
+}
+
+extern "C" int hostcheck_mgpu(int L, int n, int sign, const void *in, void *out, long long B)
+{
+    ensure_host_tables();
+    if (n < 1 || L % n) return -1;
+    const cx<double> *x = (const cx<double> *)in;
+    cx<double> *y = (cx<double> *)out;
+#define HC_MG(LL)                                                          \
+    if (L == LL) {                                                         \
+        if (sign < 0) emulate_mgpu<LL, -1>(n, x, y, B);                    \
+        else emulate_mgpu<LL, +1>(n, x, y, B);                             \
+        return 0;                                                          \
+    }
+    HC_MG(36) HC_MG(45) HC_MG(64)
+#undef HC_MG
     return -2;
 }
 

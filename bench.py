@@ -346,19 +346,24 @@ def measure_mixed(fb, torch, device, stream, peak, steps, warmup, world):
         segs64.append({"shape": shape, "batch": n, "direction": fb.FORWARD, "precision": fb.C64,
                        "in": a.data_ptr(), "out": b.data_ptr()})
         plans128.append((fb.Plan(shape, n, fb.FORWARD, fb.C128), a2, b2))
-    batch = fb.Batch(segs64)
+    batch = fb.Batch(segs64)  # the timed choice between the two strategies
+    persistent = fb.Batch(segs64, flags=fb.BATCH_PERSISTENT)
     s = stream.cuda_stream
 
     def run_batch():
         batch.execute(s)
 
+    def run_persistent():
+        persistent.execute(s)
+
     def run_plain():
         for p, a2, b2 in plans128:
             p.execute(a2.data_ptr(), b2.data_ptr(), s)
 
-    out = {"label": "uneven complex64 mix (17,216 volumes, 8 geometries), one persistent launch",
-           "batch": batch.describe()}
-    for name, fn in (("batch", run_batch), ("plain_c128", run_plain)):
+    out = {"label": "uneven complex64 mix (17,216 volumes, 8 geometries), one graph launch "
+                    "(autotuned: persistent descriptor-list kernel or per-segment plans)",
+           "batch": batch.describe(), "persistent": persistent.describe()}
+    for name, fn in (("batch", run_batch), ("persistent", run_persistent), ("plain_c128", run_plain)):
         for _ in range(warmup):
             fn()
         torch.cuda.synchronize()
@@ -376,8 +381,12 @@ def measure_mixed(fb, torch, device, stream, peak, steps, warmup, world):
     out.update({"achieved_gbs": ach, "frac": ach / peak,
                 "alg_bytes_per_launch": bytes64,
                 "speedup_vs_plain_fp64": out["batch_volumes_per_s"] / out["plain_c128_volumes_per_s"],
-                "launches_per_step": 1})
+                "persistent_speedup_vs_plain_fp64": (out["persistent_volumes_per_s"]
+                                                     / out["plain_c128_volumes_per_s"]),
+                "graph_launches_per_step": 1,
+                "kernel_launches_per_step": (len(MIX) if "one tuned plan per segment" in out["batch"] else 1)})
     batch.close()
+    persistent.close()
     del keep, plans128
     return out
 

@@ -2,8 +2,8 @@
  *
  * The six symbols of the reference contract are unchanged and live in
  * fft3d_api.h (host pointers) and fft3d_gpu_api.h (device pointers).  This header
- * adds what that contract cannot express (SURVEY of the reference: forward-only,
- * cubes only, complex double only, void returns):
+ * adds what that contract cannot express (it is forward-only, cubes only,
+ * complex double only, with void returns):
  *
  *   - anisotropic n0 x n1 x n2 extents       (python/fft3d.py:360-371 handles any shape)
  *   - direction: forward, or backward with 1/V (python/fft3d.py:402-423)
@@ -46,6 +46,8 @@ extern "C" {
 /* Plan flags. */
 #define FFT3D_B200_FLAG_NO_TUNE 0x1u   /* take the default kernel instead of timing candidates */
 #define FFT3D_B200_FLAG_NO_GRAPH 0x2u  /* batches: launch directly instead of replaying a CUDA graph */
+#define FFT3D_B200_BATCH_PERSISTENT 0x4u /* batches: always the one persistent descriptor-list kernel */
+#define FFT3D_B200_BATCH_SEGMENTS 0x8u   /* batches: always one tuned plan per segment */
 
 typedef struct fft3d_b200_plan fft3d_b200_plan;
 
@@ -147,13 +149,22 @@ typedef struct {
 
 typedef struct fft3d_b200_batch fft3d_b200_batch;
 
-/* Build a batch over `nseg` segments: validates them, uploads a descriptor list of
- * work items to the device, tunes the persistent launch and, unless
- * FFT3D_B200_FLAG_NO_GRAPH, captures it in a CUDA graph. */
+/* Build a batch over `nseg` segments.  Two launch strategies exist:
+ *   persistent -- one kernel walks a device descriptor list of work items of
+ *                 every segment (one launch for the whole batch);
+ *   segments   -- one autotuned plan per segment, the launches captured as
+ *                 parallel branches of one CUDA graph.
+ * By default both are built and timed on the batch's own buffers and the faster
+ * is kept: batch_create runs the batch a few times and so writes the segments'
+ * output buffers.  FFT3D_B200_BATCH_PERSISTENT / FFT3D_B200_BATCH_SEGMENTS pick
+ * one without timing; FFT3D_B200_FLAG_NO_TUNE takes the persistent kernel.
+ * Unless FFT3D_B200_FLAG_NO_GRAPH, the launches are replayed from a CUDA graph.
+ * With the persistent kernel every volume's result is bit-identical alone and in
+ * any mix; with per-segment plans a segment's kernel is chosen for its size. */
 int fft3d_b200_batch_create(const fft3d_b200_segment *segs, int nseg, unsigned flags, int device,
                             fft3d_b200_batch **out);
 
-/* Run every segment of the batch in one persistent launch on `stream`. */
+/* Run every segment of the batch on `stream` (one graph launch). */
 int fft3d_b200_batch_execute(fft3d_b200_batch *batch, void *stream);
 
 void fft3d_b200_batch_destroy(fft3d_b200_batch *batch);

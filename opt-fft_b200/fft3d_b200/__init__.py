@@ -39,6 +39,8 @@ C128 = 0
 C64 = 1
 FLAG_NO_TUNE = 0x1
 FLAG_NO_GRAPH = 0x2
+BATCH_PERSISTENT = 0x4
+BATCH_SEGMENTS = 0x8
 
 ELEMENT_BYTES = {C128: 16, C64: 8}
 
@@ -357,7 +359,9 @@ def batch_execute_noalloc(segments, stream: int = 0):
 
 
 class Batch:
-    """One persistent launch over segments of uneven geometry (device pointers)."""
+    """Segments of uneven geometry (device pointers) in one graph launch: the
+    persistent descriptor-list kernel or one tuned plan per segment, whichever
+    batch creation measures faster (flags BATCH_PERSISTENT / BATCH_SEGMENTS pin one)."""
 
     def __init__(self, segments, flags=0, device=-1):
         arr = _segments(segments)

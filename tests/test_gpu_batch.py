@@ -1,11 +1,13 @@
-"""The descriptor-list batch: one persistent launch over segments of uneven
-geometry, both precisions and both directions (needs a B200).
+"""Batches of uneven geometry, both precisions and both directions (needs a B200):
+the persistent descriptor-list kernel, the per-segment strategy (one tuned plan
+per segment on parallel graph branches) and the timed choice between them.
 
 Checks every compiled kind against the oracle, the full uneven complex64 mix of
 the batching configuration (6^3 x 8192 ... 36^3 x 64, 8x8x16 x 1024, with a
 seeded 10% of volumes at log-uniform magnitudes 1e-2..1e2) against the FP64
-oracle per volume, and that every volume's result is bit-identical alone and in
-the mix, with and without CUDA-graph replay.
+oracle per volume, that with the persistent kernel every volume's result is
+bit-identical alone and in the mix, with and without CUDA-graph replay, and
+that the per-segment strategy reproduces the standalone plans bit for bit.
 """
 import numpy as np
 import pytest
@@ -105,13 +107,13 @@ def test_alone_equals_mixed_and_graph_equals_direct():
             dt = np.complex128 if p == fb.C128 else np.complex64
             n = 3 if np.prod(shape) > 10000 else 13
             specs.append((shape, field(rng, (n,) + shape, "uniform", dt), fb.FORWARD, p))
-    mixed, _, mouts = make_batch(specs)
+    mixed, _, mouts = make_batch(specs, flags=fb.BATCH_PERSISTENT)
     mixed.execute()
-    direct, _, douts = make_batch(specs, flags=fb.FLAG_NO_GRAPH)
+    direct, _, douts = make_batch(specs, flags=fb.FLAG_NO_GRAPH | fb.BATCH_PERSISTENT)
     direct.execute()
     torch.cuda.synchronize()
     for k, spec in enumerate(specs):
-        alone, _, aouts = make_batch([spec])
+        alone, _, aouts = make_batch([spec], flags=fb.BATCH_PERSISTENT)
         alone.execute()
         torch.cuda.synchronize()
         assert torch.equal(aouts[0], mouts[k]), f"segment {k} differs alone vs mixed"
@@ -154,3 +156,48 @@ def test_batch_rejects_bad_segments():
     empty = fb.Batch([])
     empty.execute()
     torch.cuda.synchronize()
+
+
+def test_per_segment_strategy_matches_standalone_plans():
+    """BATCH_SEGMENTS runs one tuned plan per segment on parallel graph branches:
+    each segment must equal the same plan run alone, and the oracle."""
+    rng = np.random.default_rng(23)
+    specs = []
+    for shape in KINDS:
+        for p in (fb.C128, fb.C64):
+            dt = np.complex128 if p == fb.C128 else np.complex64
+            n = 3 if np.prod(shape) > 10000 else 21
+            specs.append((shape, field(rng, (n,) + shape, "uniform", dt),
+                          fb.FORWARD if len(specs) % 2 == 0 else fb.BACKWARD, p))
+    for flags in (fb.BATCH_SEGMENTS, fb.BATCH_SEGMENTS | fb.FLAG_NO_GRAPH):
+        batch, ins, outs = make_batch(specs, flags=flags)
+        assert "one tuned plan per segment" in batch.describe()
+        batch.execute()
+        torch.cuda.synchronize()
+        for k, (shape, x, d, p) in enumerate(specs):
+            plan = fb.Plan(shape, x.shape[0], d, p)
+            alone = torch.empty_like(ins[k])
+            plan.execute(ins[k].data_ptr(), alone.data_ptr())
+            torch.cuda.synchronize()
+            assert torch.equal(alone, outs[k]), f"segment {k} differs from its plan alone"
+            err = oracle.rel_error_per_volume(outs[k].cpu().numpy().astype(np.complex128), ref(x, d))
+            assert err.max() < (C128_TOL if p == fb.C128 else C64_TOL), (shape, p, err.max())
+
+
+def test_timed_choice_is_reported_and_correct():
+    """Default flags: both strategies are built and timed; the description says
+    which won and the result matches the oracle either way."""
+    rng = np.random.default_rng(29)
+    specs = [((8, 8, 8), field(rng, (600, 8, 8, 8), "uniform", np.complex64), fb.FORWARD, fb.C64),
+             ((17, 17, 17), field(rng, (40, 17, 17, 17), "uniform", np.complex64), fb.FORWARD, fb.C64),
+             ((36, 36, 36), field(rng, (4, 36, 36, 36), "uniform", np.complex128), fb.BACKWARD, fb.C128)]
+    batch, ins, outs = make_batch(specs)
+    assert "timed: per-segment" in batch.describe(), batch.describe()
+    # the race ran the batch on these buffers; run it again on fresh outputs
+    for o in outs:
+        o.zero_()
+    batch.execute()
+    torch.cuda.synchronize()
+    for k, (shape, x, d, p) in enumerate(specs):
+        err = oracle.rel_error_per_volume(outs[k].cpu().numpy().astype(np.complex128), ref(x, d))
+        assert err.max() < (C128_TOL if p == fb.C128 else C64_TOL), (shape, err.max())

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "mgpu.cuh"
+#include "splitline.cuh"
 #include "twopass.cuh"
 #include "volume.cuh"
 
@@ -173,7 +174,87 @@ static void emulate_twopass(const void *vin, void *vout, long long nvol)
     }
 }
 
+// The split-line TWOPASS variant (SPLIT = true): every pass whose length has a
+// lane split runs split_line_host over whole lines, the host form of the
+// kernel's lane exchange; other axes keep the one-thread-per-line pass.
+template <int N, int S, typename T, class Ld, class St>
+static void line_any(Ld ld, St st)
+{
+    if constexpr (LineSplit<N>::P > 1) {
+        split_line_host<N, S, T>(ld, st);
+    } else {
+        cx<T> v[N];
+        for (int j = 0; j < N; ++j) v[j] = ld(j);
+        dft<N, S, T>(v);
+        for (int j = 0; j < N; ++j) st(j, v[j]);
+    }
+}
+
+template <int N0, int N1, int N2, typename T, int S, int G>
+static void emulate_twopass_split(const void *vin, void *vout, long long nvol)
+{
+    using TG = TwoPassGeom<N0, N1, N2, T, G>;
+    using XG = typename TG::XG;
+    using YG = typename TG::YG;
+    const T scale = S > 0 ? T(1) / T(TG::V) : T(1);
+    int lag = 0;
+    const int R = twopass_ring_size(TG::NA, TG::NB, 7, &lag);
+    std::vector<cx<T>> sm((size_t)TG::PV), ring((size_t)R * TG::V, cx<T>{T(-777.0), T(555.0)});
+    const cx<T> *in = (const cx<T> *)vin;
+    cx<T> *out = (cx<T> *)vout;
+    const long long total = (long long)(TG::NA + TG::NB) * nvol;
+    for (long long t = 0; t < total; ++t) {
+        const TwoPassItem it = twopass_decode(t, nvol, TG::NA, TG::NB, lag);
+        cx<T> *sv = ring.data() + (it.vol % R) * TG::V;
+        for (auto &e : sm) e = {T(12345.0), T(-6789.0)};
+        cx<T> *s = sm.data();
+        if (it.plane) {
+            for (int g = 0; g < TG::PLANE_ELEMS; ++g) {
+                long long vo;
+                int so;
+                twopass_plane_elem<TG>(it.j, g, &vo, &so);
+                s[so] = in[it.vol * TG::V + vo];
+            }
+            for (int r = 0; r < XG::ROWS; ++r)
+                line_any<N2, S, T>([&](int z) { return s[XG::off(r, z)]; },
+                                   [&](int z, cx<T> v) { s[XG::off(r, z)] = v; });
+            for (int l = 0; l < G * N2; ++l) {
+                const int z = l % N2, rb = (l / N2) * N1;
+                line_any<N1, S, T>([&](int y) { return s[XG::off(rb + y, z)]; },
+                                   [&](int y, cx<T> v) { s[XG::off(rb + y, z)] = v; });
+            }
+            for (int g = 0; g < TG::PLANE_ELEMS; ++g) {
+                long long vo;
+                int so;
+                twopass_plane_elem<TG>(it.j, g, &vo, &so);
+                sv[vo] = s[so];
+            }
+        } else {
+            for (int g = 0; g < TG::ROW_ELEMS; ++g) {
+                long long vo;
+                int so;
+                twopass_row_elem<TG>(it.j, g, &vo, &so);
+                s[so] = sv[vo];
+            }
+            cx<T> *gvol = out + it.vol * TG::V;
+            for (int l = 0; l < G * N2; ++l) {
+                const int z = l % N2, y = l / N2;
+                line_any<N0, S, T>([&](int j) { return s[YG::off(j * G + y, z)]; },
+                                   [&](int j, cx<T> v) {
+                                       if (S > 0) v = cscale(v, scale);
+                                       gvol[((long long)j * N1 + it.j * G + y) * N2 + z] = v;
+                                   });
+            }
+        }
+    }
+}
+
 typedef void (*emu_fn)(const void *, void *, long long);
+
+#define EMU_TPS(N0, N1, N2, T, G)                                                             \
+    {N0, N1, N2, sizeof(T) == 8 ? 0 : 1, -1, 400 + G, 1,                                    \
+     &emulate_twopass_split<N0, N1, N2, T, -1, G>},                                          \
+    {N0, N1, N2, sizeof(T) == 8 ? 0 : 1, +1, 400 + G, 1, &emulate_twopass_split<N0, N1, N2, T, +1, G>}
 
 #define EMU_TP(N0, N1, N2, T, G)                                                              \
     {N0, N1, N2, sizeof(T) == 8 ? 0 : 1, -1, 300 + G, 1,                                    \
@@ -219,6 +300,8 @@ static const EmuEntry kEmu[] = {
     EMU(13, 13, 13, double, 0, 2), EMU(23, 23, 23, double, 0, 1),  EMU(13, 13, 13, float, 0, 4),
     EMU(23, 23, 23, float, 0, 1),  EMU_TP(45, 45, 45, double, 3), EMU_TP(45, 45, 45, float, 5),
     EMU_TP(64, 64, 64, double, 1), EMU_TP(64, 64, 64, float, 2),
+    EMU_TPS(36, 36, 36, double, 2), EMU_TPS(36, 36, 36, double, 1), EMU_TPS(36, 36, 36, float, 4),
+    EMU_TPS(64, 64, 64, double, 1), EMU_TPS(64, 64, 64, float, 2),  EMU_TPS(36, 36, 64, double, 2),
 };
 
 // The chain kernel's per-CTA loop (chain_kernels.cu k_chain) for one volume per CTA.

@@ -118,6 +118,13 @@ __device__ __forceinline__ void fence_proxy_async_smem()
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
+// Order this thread's generic-proxy view of global memory (e.g. an acquire that
+// found another CTA's data published) before its later async-proxy (TMA) reads.
+__device__ __forceinline__ void fence_proxy_async_global()
+{
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
 // One-dimensional bulk copy global -> shared (TMA, no tensor map), completing
 // `bytes` of transaction count on `bar`.  dst, src 16-byte aligned; bytes % 16 == 0.
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)

@@ -19,6 +19,7 @@
 // launch, on the error path as well.
 #include "internal.h"
 #include "ptx.cuh"
+#include "splitline.cuh"
 #include "twopass.cuh"
 
 namespace fft3d {
@@ -42,7 +43,87 @@ __device__ __forceinline__ void st_l2(cx<T> *p, cx<T> v)
     else __stcg(reinterpret_cast<float2 *>(p), make_float2(v.re, v.im));
 }
 
-template <int N0, int N1, int N2, typename T, int S, int G, int NT, int MINB>
+// The three passes with each line spread over P = LineSplit<N>::P lanes
+// (splitline.cuh); axes whose length has no split keep one thread per line.
+// Every lane of the CTA runs the same number of rounds, so whole warps reach
+// each shuffle; P consecutive tasks are the P lanes of one line.
+template <class XG, int S, int NT>
+__device__ __forceinline__ void tp_pass_z(cx<typename XG::T> *sm, int tid)
+{
+    using T = typename XG::T;
+    constexpr int N = XG::N2, P = LineSplit<N>::P;
+    if constexpr (P == 1) {
+        for (int r = tid; r < XG::ROWS; r += NT) pass_z<XG, S, ALG_DEFAULT>(sm, r);
+    } else {
+        static_assert(NT % 32 == 0, "whole warps");
+        constexpr int TASKS = XG::ROWS * P;
+        for (int base = 0; base < TASKS; base += NT) {
+            const int task = base + tid;
+            const bool valid = task < TASKS;
+            const int r = valid ? task / P : 0, t = task % P;
+            split_line<N, S, T>(t, valid, [&](int z) { return sm[XG::off(r, z)]; },
+                                [&](int z, cx<T> v) { sm[XG::off(r, z)] = v; });
+        }
+    }
+}
+
+template <class XG, int S, int NT>
+__device__ __forceinline__ void tp_pass_y(cx<typename XG::T> *sm, int tid)
+{
+    using T = typename XG::T;
+    constexpr int N = XG::N1, P = LineSplit<N>::P;
+    constexpr int LINES = XG::N0 * XG::N2;
+    if constexpr (P == 1) {
+        for (int l = tid; l < LINES; l += NT) pass_y<XG, S, ALG_DEFAULT>(sm, l);
+    } else {
+        static_assert(NT % 32 == 0, "whole warps");
+        constexpr int TASKS = LINES * P;
+        for (int base = 0; base < TASKS; base += NT) {
+            const int task = base + tid;
+            const bool valid = task < TASKS;
+            const int l = valid ? task / P : 0, t = task % P;
+            const int z = l % XG::N2, rb = (l / XG::N2) * XG::N1;
+            split_line<N, S, T>(t, valid, [&](int y) { return sm[XG::off(rb + y, z)]; },
+                                [&](int y, cx<T> v) { sm[XG::off(rb + y, z)] = v; });
+        }
+    }
+}
+
+// x pass of a row item: YG holds G y-rows of all N0 planes; results go to gvol.
+template <class YG, int S, int GN1, int NT>
+__device__ __forceinline__ void tp_pass_x(const cx<typename YG::T> *sm, int tid, cx<typename YG::T> *gvol,
+                                          int y0, typename YG::T scale)
+{
+    using T = typename YG::T;
+    constexpr int N = YG::N0, P = LineSplit<N>::P;
+    constexpr int LINES = YG::N1 * YG::N2;
+    if constexpr (P == 1) {
+        for (int l = tid; l < LINES; l += NT) pass_x_slab<YG, S, GN1>(sm, l, gvol, y0, scale);
+    } else {
+        static_assert(NT % 32 == 0, "whole warps");
+        constexpr int TASKS = LINES * P;
+        for (int base = 0; base < TASKS; base += NT) {
+            const int task = base + tid;
+            const bool valid = task < TASKS;
+            const int l = valid ? task / P : 0, t = task % P;
+            const int z = l % YG::N2, y = l / YG::N2;
+            split_line<N, S, T>(
+                t, valid, [&](int j) { return sm[YG::off(j * YG::N1 + y, z)]; },
+                [&](int j, cx<T> v) {
+                    if constexpr (S > 0) v = cscale(v, scale);
+                    store_out(gvol + ((long long)j * GN1 + y0 + y) * YG::N2 + z, v);
+                });
+        }
+    }
+}
+
+// BULK (complex double): every row of N2 points is moved by one bulk copy
+// (cp.async.bulk, completing on an mbarrier with a bounded wait) -- the plane
+// rows from the input, the row-item rows from scratch -- and the scratch store
+// walks whole rows, one warp per row: no per-element index arithmetic, which
+// otherwise costs more instructions than the transform itself.
+template <int N0, int N1, int N2, typename T, int S, int G, int NT, int MINB, bool SPLIT,
+          bool BULK = false>
 __global__ void __launch_bounds__(NT, MINB)
     k_twopass(const cx<T> *__restrict__ in, cx<T> *__restrict__ out, long long nvol, T scale,
               int *err, unsigned char *work, int R, int D)
@@ -50,15 +131,28 @@ __global__ void __launch_bounds__(NT, MINB)
     using TG = TwoPassGeom<N0, N1, N2, T, G>;
     using XG = typename TG::XG;
     using YG = typename TG::YG;
+    static_assert(!BULK || (sizeof(T) == 8 && XG::POL != 2 && NT % 32 == 0),
+                  "bulk rows: complex double, row-major layouts, whole warps");
     constexpr int U = 8;  // L2 loads in flight per thread in the row gather
+    constexpr uint32_t ROW_BYTES = (uint32_t)(N2 * sizeof(cx<T>));
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);
     __shared__ long long s_t;
     __shared__ int s_stop;
+    __shared__ __align__(8) uint64_t s_bar;
     TwoPassCtl *ctl = reinterpret_cast<TwoPassCtl *>(work);
     cx<T> *ring = reinterpret_cast<cx<T> *>(work + TWOPASS_CTL_BYTES);
     const int tid = threadIdx.x;
     const long long total = (long long)(TG::NA + TG::NB) * nvol;
+    uint32_t phase = 0;
+    bool copies_pending = false;
+    if constexpr (BULK) {
+        if (tid == 0) {
+            mbar_init(&s_bar, 1);
+            fence_mbar_init();
+        }
+        __syncthreads();
+    }
 
     for (;;) {
         if (tid == 0) {
@@ -76,20 +170,40 @@ __global__ void __launch_bounds__(NT, MINB)
         if (it.plane) {
             // 1. G contiguous planes of the input
             const cx<T> *src = in + it.vol * TG::V;
-            for (int g = tid; g < TG::PLANE_ELEMS; g += NT) {
-                long long vo;
-                int so;
-                twopass_plane_elem<TG>(it.j, g, &vo, &so);
-                if constexpr (sizeof(T) == 8) cp_async_16(sm + so, src + vo);
-                else cp_async_8(sm + so, src + vo);
+            if constexpr (BULK) {
+                if (tid == 0) mbar_arrive_expect_tx(&s_bar, (uint32_t)XG::ROWS * ROW_BYTES);
+                const cx<T> *rows = src + (long long)it.j * G * N1 * N2;
+                for (int r = tid; r < XG::ROWS; r += NT)
+                    bulk_g2s(sm + XG::off(r, 0), rows + (long long)r * N2, ROW_BYTES, &s_bar);
+                copies_pending = true;
+                const bool ok = mbar_wait_bounded(&s_bar, phase);
+                phase ^= 1u;
+                if (!ok && tid == 0) s_stop = 2;
+                if (ok) copies_pending = false;
+                __syncthreads();
+                if (s_stop) break;
+            } else {
+                for (int g = tid; g < TG::PLANE_ELEMS; g += NT) {
+                    long long vo;
+                    int so;
+                    twopass_plane_elem<TG>(it.j, g, &vo, &so);
+                    if constexpr (sizeof(T) == 8) cp_async_16(sm + so, src + vo);
+                    else cp_async_8(sm + so, src + vo);
+                }
+                cp_async_commit();
+                cp_async_wait<0>();
+                __syncthreads();
             }
-            cp_async_commit();
-            cp_async_wait<0>();
-            __syncthreads();
             // 2. z and y passes
-            for (int r = tid; r < G * N1; r += NT) pass_z<XG, S, ALG_DEFAULT>(sm, r);
-            __syncthreads();
-            for (int l = tid; l < G * N2; l += NT) pass_y<XG, S, ALG_DEFAULT>(sm, l);
+            if constexpr (SPLIT) {
+                tp_pass_z<XG, S, NT>(sm, tid);
+                __syncthreads();
+                tp_pass_y<XG, S, NT>(sm, tid);
+            } else {
+                for (int r = tid; r < G * N1; r += NT) pass_z<XG, S, ALG_DEFAULT>(sm, r);
+                __syncthreads();
+                for (int l = tid; l < G * N2; l += NT) pass_y<XG, S, ALG_DEFAULT>(sm, l);
+            }
             // 3. the slot's previous volume must have been read out
             if (tid == 0)
                 s_stop = wait_counter_geq(&ctl->cnt[TWOPASS_RMAX + slot], (unsigned)TG::NB * round,
@@ -99,11 +213,17 @@ __global__ void __launch_bounds__(NT, MINB)
             __syncthreads();
             if (s_stop) break;
             // 4. to scratch, same offsets as in the volume, L2 only
-            for (int g = tid; g < TG::PLANE_ELEMS; g += NT) {
-                long long vo;
-                int so;
-                twopass_plane_elem<TG>(it.j, g, &vo, &so);
-                st_l2(sv + vo, sm[so]);
+            if constexpr (BULK) {
+                cx<T> *rows = sv + (long long)it.j * G * N1 * N2;
+                for (int r = tid / 32; r < XG::ROWS; r += NT / 32)
+                    for (int z = tid % 32; z < N2; z += 32) st_l2(rows + (long long)r * N2 + z, sm[XG::off(r, z)]);
+            } else {
+                for (int g = tid; g < TG::PLANE_ELEMS; g += NT) {
+                    long long vo;
+                    int so;
+                    twopass_plane_elem<TG>(it.j, g, &vo, &so);
+                    st_l2(sv + vo, sm[so]);
+                }
             }
             __threadfence();
             __syncthreads();
@@ -116,7 +236,23 @@ __global__ void __launch_bounds__(NT, MINB)
                              : 1;
             __syncthreads();
             if (s_stop) break;
-            // 2. gather the G rows of every plane, U loads in flight per thread
+            // 2. gather the G rows of every plane
+            if constexpr (BULK) {
+                if (tid == 0) mbar_arrive_expect_tx(&s_bar, (uint32_t)(N0 * G) * ROW_BYTES);
+                for (int q = tid; q < N0 * G; q += NT) {
+                    const int x = q / G, yl = q % G;
+                    fence_proxy_async_global();  // the acquire above precedes these TMA reads
+                    bulk_g2s(sm + YG::off(q, 0), sv + ((long long)x * N1 + it.j * G + yl) * N2, ROW_BYTES,
+                             &s_bar);
+                }
+                copies_pending = true;
+                const bool ok = mbar_wait_bounded(&s_bar, phase);
+                phase ^= 1u;
+                if (!ok && tid == 0) s_stop = 2;
+                if (ok) copies_pending = false;
+                __syncthreads();
+                if (s_stop) break;
+            } else
             for (int base = 0; base < TG::ROW_ELEMS; base += NT * U) {
                 cx<T> v[U];
                 int so[U];
@@ -139,9 +275,16 @@ __global__ void __launch_bounds__(NT, MINB)
             if (tid == 0) red_release_gpu_add(&ctl->cnt[TWOPASS_RMAX + slot], 1u);
             // 3. x pass, straight to the output
             cx<T> *gvol = out + it.vol * TG::V;
-            for (int l = tid; l < G * N2; l += NT) pass_x_slab<YG, S, N1>(sm, l, gvol, it.j * G, scale);
+            if constexpr (SPLIT) tp_pass_x<YG, S, N1, NT>(sm, tid, gvol, it.j * G, scale);
+            else
+                for (int l = tid; l < G * N2; l += NT) pass_x_slab<YG, S, N1>(sm, l, gvol, it.j * G, scale);
         }
+        if constexpr (BULK) fence_proxy_async_smem();  // generic reads before the next TMA writes
         __syncthreads();  // the next item reuses shared memory
+    }
+    // a bulk copy that timed out may still land: wait once more (bounded)
+    if constexpr (BULK) {
+        if (copies_pending) mbar_wait_bounded(&s_bar, phase ^ 1u);
     }
 
     // A wait that timed out: record it and stop the other CTAs.
@@ -164,6 +307,148 @@ __global__ void __launch_bounds__(NT, MINB)
     }
 }
 
+// Pipelined TWOPASS (complex double): two shared-memory stages per CTA; while
+// one item is transformed, the next item's copies are in flight.  The next
+// ticket is taken at the top of each iteration; its load is issued at once when
+// it can start -- a plane item always (its input is read-only), a row item only
+// when a non-blocking check finds its volume's plane items done -- and
+// otherwise after the current item, with a blocking wait.  A CTA therefore
+// blocks only on the dependencies of its single unfinished item, as in
+// k_twopass, and the ticket-order argument against deadlock still holds.
+// Row items read scratch with cp.async.cg (L2 only, never a stale L1 line).
+template <int N0, int N1, int N2, int S, int G, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
+    k_twopass_pipe(const cx<double> *__restrict__ in, cx<double> *__restrict__ out, long long nvol,
+                   double scale, int *err, unsigned char *work, int R, int D)
+{
+    using T = double;
+    using TG = TwoPassGeom<N0, N1, N2, T, G>;
+    using XG = typename TG::XG;
+    using YG = typename TG::YG;
+    constexpr int STAGE = TG::SMEM;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ long long s_tk[2];
+    __shared__ int s_next;  // 1: next item's load issued, 0: deferred, -1: no next item
+    __shared__ int s_stop;
+    TwoPassCtl *ctl = reinterpret_cast<TwoPassCtl *>(work);
+    cx<T> *ring = reinterpret_cast<cx<T> *>(work + TWOPASS_CTL_BYTES);
+    const int tid = threadIdx.x;
+    const long long total = (long long)(TG::NA + TG::NB) * nvol;
+    auto stage = [&](int s) { return reinterpret_cast<cx<T> *>(smraw + s * STAGE); };
+    auto issue = [&](const TwoPassItem &it, int s) {
+        cx<T> *sm = stage(s);
+        if (it.plane) {
+            const cx<T> *src = in + it.vol * TG::V;
+            for (int g = tid; g < TG::PLANE_ELEMS; g += NT) {
+                long long vo;
+                int so;
+                twopass_plane_elem<TG>(it.j, g, &vo, &so);
+                cp_async_16(sm + so, src + vo);
+            }
+        } else {
+            const cx<T> *sv = ring + (it.vol % R) * TG::V;
+            for (int g = tid; g < TG::ROW_ELEMS; g += NT) {
+                long long vo;
+                int so;
+                twopass_row_elem<TG>(it.j, g, &vo, &so);
+                cp_async_16(sm + so, sv + vo);
+            }
+        }
+        cp_async_commit();
+    };
+    auto plane_target = [&](const TwoPassItem &it) { return (unsigned)TG::NA * (unsigned)(it.vol / R + 1); };
+
+    int cur = 0;
+    if (tid == 0) {
+        const long long t = (long long)atomicAdd(&ctl->ticket, 1ull);
+        s_tk[0] = t;
+        s_stop = (t >= total || ld_acquire_gpu(&ctl->abort) != 0) ? 1 : 0;
+        if (!s_stop) {
+            const TwoPassItem it = twopass_decode(t, nvol, TG::NA, TG::NB, D);
+            if (!it.plane && !wait_counter_geq(&ctl->cnt[it.vol % R], plane_target(it), &ctl->abort))
+                s_stop = 2;
+        }
+    }
+    __syncthreads();
+    if (s_stop == 0) issue(twopass_decode(s_tk[0], nvol, TG::NA, TG::NB, D), 0);
+
+    while (s_stop == 0) {
+        const TwoPassItem it = twopass_decode(s_tk[cur], nvol, TG::NA, TG::NB, D);
+        const int slot = (int)(it.vol % R);
+        if (tid == 0) {
+            const long long t = (long long)atomicAdd(&ctl->ticket, 1ull);
+            s_tk[cur ^ 1] = t;
+            int st = -1;
+            if (t < total && ld_acquire_gpu(&ctl->abort) == 0) {
+                const TwoPassItem nx = twopass_decode(t, nvol, TG::NA, TG::NB, D);
+                st = (nx.plane || ld_acquire_gpu(&ctl->cnt[nx.vol % R]) >= plane_target(nx)) ? 1 : 0;
+            }
+            s_next = st;
+        }
+        __syncthreads();
+        const int nstate = s_next;
+        if (nstate == 1) issue(twopass_decode(s_tk[cur ^ 1], nvol, TG::NA, TG::NB, D), cur ^ 1);
+        if (nstate == 1) cp_async_wait<1>();
+        else cp_async_wait<0>();
+        __syncthreads();
+        cx<T> *sm = stage(cur);
+        cx<T> *sv = ring + (long long)slot * TG::V;
+        if (it.plane) {
+            for (int r = tid; r < G * N1; r += NT) pass_z<XG, S, ALG_DEFAULT>(sm, r);
+            __syncthreads();
+            for (int l = tid; l < G * N2; l += NT) pass_y<XG, S, ALG_DEFAULT>(sm, l);
+            if (tid == 0 && !wait_counter_geq(&ctl->cnt[TWOPASS_RMAX + slot],
+                                              (unsigned)TG::NB * (unsigned)(it.vol / R), &ctl->abort))
+                s_stop = 2;
+            __syncthreads();
+            if (s_stop) break;
+            for (int g = tid; g < TG::PLANE_ELEMS; g += NT) {
+                long long vo;
+                int so;
+                twopass_plane_elem<TG>(it.j, g, &vo, &so);
+                st_l2(sv + vo, sm[so]);
+            }
+            __threadfence();
+            __syncthreads();
+            if (tid == 0) red_release_gpu_add(&ctl->cnt[slot], 1u);
+        } else {
+            // the copies of this row item are complete: its slot may be reused
+            if (tid == 0) red_release_gpu_add(&ctl->cnt[TWOPASS_RMAX + slot], 1u);
+            cx<T> *gvol = out + it.vol * TG::V;
+            for (int l = tid; l < G * N2; l += NT) pass_x_slab<YG, S, N1>(sm, l, gvol, it.j * G, scale);
+        }
+        __syncthreads();  // stage `cur` is free again
+        if (nstate == -1) break;
+        if (nstate == 0) {
+            const TwoPassItem nx = twopass_decode(s_tk[cur ^ 1], nvol, TG::NA, TG::NB, D);
+            if (tid == 0 && !wait_counter_geq(&ctl->cnt[nx.vol % R], plane_target(nx), &ctl->abort))
+                s_stop = 2;
+            __syncthreads();
+            if (s_stop) break;
+            issue(nx, cur ^ 1);
+        }
+        cur ^= 1;
+    }
+    cp_async_wait<0>();  // no copy in flight when the CTA leaves
+
+    if (tid == 0 && s_stop == 2) {
+        report_error(err, DEV_ERR_DEP_TIMEOUT);
+        atomicExch(&ctl->abort, 1u);
+    }
+    if (tid == 0) {
+        __threadfence();
+        const unsigned prev = atomicAdd(&ctl->done, 1u);
+        if (prev == gridDim.x - 1) {
+            __threadfence();
+            ctl->ticket = 0ull;
+            for (int i = 0; i < 2 * TWOPASS_RMAX; ++i) ctl->cnt[i] = 0u;
+            ctl->abort = 0u;
+            __threadfence();
+            ctl->done = 0u;
+        }
+    }
+}
+
 int twopass_ring(const KernelEntry &e, long long grid, int *lag)
 {
     return twopass_ring_size(e.n0 / e.vpc, e.n1 / e.vpc, grid, lag);
@@ -177,7 +462,8 @@ size_t entry_workspace_bytes(const KernelEntry &e, int grid_limit)
     return TWOPASS_CTL_BYTES + (size_t)r * (size_t)e.n0 * e.n1 * e.n2 * (size_t)element_bytes(e.precision);
 }
 
-template <int N0, int N1, int N2, typename T, int S, int G, int NT, int MINB>
+template <int N0, int N1, int N2, typename T, int S, int G, int NT, int MINB, bool SPLIT = false,
+          bool BULK = false>
 static void add_twopass(std::vector<KernelEntry> &out, const char *name)
 {
     KernelEntry e;
@@ -187,11 +473,11 @@ static void add_twopass(std::vector<KernelEntry> &out, const char *name)
     e.precision = sizeof(T) == 8 ? FFT3D_B200_C128 : FFT3D_B200_C64;
     e.sign = S;
     e.family = FAM_TWOPASS;
-    e.alg = 0;
     e.vpc = G;
     e.threads = NT;
     e.smem = TwoPassGeom<N0, N1, N2, T, G>::SMEM;
-    e.func = (const void *)&k_twopass<N0, N1, N2, T, S, G, NT, MINB>;
+    e.alg = (SPLIT ? 1 : 0) + (BULK ? 4 : 0);
+    e.func = (const void *)&k_twopass<N0, N1, N2, T, S, G, NT, MINB, SPLIT, BULK>;
     e.name = name;
     out.push_back(e);
 }
@@ -202,8 +488,71 @@ static void add_twopass(std::vector<KernelEntry> &out, const char *name)
     add_twopass<N0, N1, N2, T, +1, G, NT, MINB>(out, "twopass " #N0 "x" #N1 "x" #N2 " " #T    \
                                                      " g" #G " nt" #NT " minb" #MINB)
 
+template <int N0, int N1, int N2, int S, int G, int NT, int MINB>
+static void add_twopass_pipe(std::vector<KernelEntry> &out, const char *name)
+{
+    KernelEntry e;
+    e.n0 = N0;
+    e.n1 = N1;
+    e.n2 = N2;
+    e.precision = FFT3D_B200_C128;
+    e.sign = S;
+    e.family = FAM_TWOPASS;  // same launch arguments and workspace as k_twopass
+    e.alg = 2;
+    e.vpc = G;
+    e.threads = NT;
+    e.smem = 2 * TwoPassGeom<N0, N1, N2, double, G>::SMEM;
+    e.func = (const void *)&k_twopass_pipe<N0, N1, N2, S, G, NT, MINB>;
+    e.name = name;
+    out.push_back(e);
+}
+
+// Rows moved by bulk copies (complex double, row-major layouts): "bulk" in the name.
+#define FFT3D_TWOPASS_BULK(N0, N1, N2, G, NT, MINB)                                              \
+    add_twopass<N0, N1, N2, double, -1, G, NT, MINB, false, true>(                               \
+        out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G " bulk nt" #NT " minb" #MINB);        \
+    add_twopass<N0, N1, N2, double, +1, G, NT, MINB, false, true>(                               \
+        out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G " bulk nt" #NT " minb" #MINB)
+
+// Two-stage pipeline, complex double: "pipe" in the name.
+#define FFT3D_TWOPASS_PIPE(N0, N1, N2, G, NT, MINB)                                              \
+    add_twopass_pipe<N0, N1, N2, -1, G, NT, MINB>(out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G \
+                                                       " pipe nt" #NT " minb" #MINB);              \
+    add_twopass_pipe<N0, N1, N2, +1, G, NT, MINB>(out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G \
+                                                       " pipe nt" #NT " minb" #MINB)
+
+// Lines split over P lanes (splitline.cuh): "split" in the name.
+#define FFT3D_TWOPASS_SPLIT(N0, N1, N2, T, G, NT, MINB)                                          \
+    add_twopass<N0, N1, N2, T, -1, G, NT, MINB, true>(out, "twopass " #N0 "x" #N1 "x" #N2 " " #T \
+                                                           " g" #G " split nt" #NT " minb" #MINB); \
+    add_twopass<N0, N1, N2, T, +1, G, NT, MINB, true>(out, "twopass " #N0 "x" #N1 "x" #N2 " " #T \
+                                                           " g" #G " split nt" #NT " minb" #MINB)
+
 void register_twopass_kernels(std::vector<KernelEntry> &out)
 {
+    // rows moved by bulk copies: almost no integer work outside the transform
+    FFT3D_TWOPASS_BULK(36, 36, 36, 2, 96, 4);
+    FFT3D_TWOPASS_BULK(36, 36, 36, 4, 160, 2);
+    FFT3D_TWOPASS_BULK(36, 36, 36, 1, 64, 6);
+    FFT3D_TWOPASS_BULK(45, 45, 45, 3, 160, 2);
+    FFT3D_TWOPASS_BULK(45, 45, 45, 5, 256, 1);
+    // two stages per CTA: the next item's copies overlap the current transform
+    FFT3D_TWOPASS_PIPE(36, 36, 36, 2, 96, 2);
+    FFT3D_TWOPASS_PIPE(36, 36, 36, 1, 64, 5);
+    FFT3D_TWOPASS_PIPE(36, 36, 36, 1, 64, 4);
+    FFT3D_TWOPASS_PIPE(36, 36, 36, 4, 160, 1);
+    FFT3D_TWOPASS_PIPE(16, 16, 32, 4, 128, 3);
+    FFT3D_TWOPASS_PIPE(16, 16, 32, 2, 64, 6);
+    // 36^3 and 64^3 with lines split over 4 lanes: about 70 registers a lane
+    FFT3D_TWOPASS_SPLIT(36, 36, 36, double, 2, 288, 2);
+    FFT3D_TWOPASS_SPLIT(36, 36, 36, double, 4, 576, 1);
+    FFT3D_TWOPASS_SPLIT(36, 36, 36, double, 1, 160, 4);
+    FFT3D_TWOPASS_SPLIT(36, 36, 36, float, 4, 576, 1);
+    FFT3D_TWOPASS_SPLIT(36, 36, 36, float, 2, 288, 3);
+    FFT3D_TWOPASS_SPLIT(64, 64, 64, double, 1, 256, 2);
+    FFT3D_TWOPASS_SPLIT(64, 64, 64, double, 2, 512, 1);
+    FFT3D_TWOPASS_SPLIT(64, 64, 64, float, 2, 512, 1);
+    FFT3D_TWOPASS_SPLIT(64, 64, 64, float, 1, 256, 3);
     // 36^3: 36 lines per plane or row, one thread per line
     FFT3D_TWOPASS(36, 36, 36, double, 4, 160, 2);
     FFT3D_TWOPASS(36, 36, 36, double, 2, 96, 4);

@@ -126,6 +126,27 @@ def test_twopass_items(hostcheck, shape, prec, g, nvol, sign):
     assert err < (C128_TOL if prec == 0 else C64_TOL), err
 
 
+SPLIT = [((36, 36, 36), 0, 2, 11), ((36, 36, 36), 0, 1, 3), ((36, 36, 36), 1, 4, 5),
+         ((64, 64, 64), 0, 1, 3), ((64, 64, 64), 1, 2, 2), ((36, 36, 64), 0, 2, 4)]
+
+
+@pytest.mark.parametrize("shape,prec,g,nvol", SPLIT,
+                         ids=[f"{t[0]}-c{128 if t[1] == 0 else 64}-g{t[2]}-b{t[3]}" for t in SPLIT])
+@pytest.mark.parametrize("sign", [-1, +1])
+def test_twopass_split_lines(hostcheck, shape, prec, g, nvol, sign):
+    """TWOPASS with 36- and 64-point lines spread over 4 lanes (alg = 400 + G):
+    the Good-Thomas (36 = 4 x 9) and Cooley-Tukey (64 = 4 x 16) index maps and
+    the radix-2 lane exchange, in the host form of the kernel's shuffles."""
+    rng = np.random.default_rng(6000 + g + nvol + prec + sum(shape))
+    dt = np.complex128 if prec == 0 else np.complex64
+    x = field(rng, (nvol,) + shape, dist="normal", dtype=dt)
+    got = run(hostcheck, x, shape, prec, sign, 400 + g, 1)
+    x64 = x.astype(np.complex128)
+    want = oracle.fft3d(x64) if sign < 0 else oracle.ifft3d(x64)
+    err = oracle.rel_error_per_volume(got, want).max()
+    assert err < (C128_TOL if prec == 0 else C64_TOL), err
+
+
 GOLD = [p for p in sorted(glob.glob(os.path.join(GOLDEN, "vol_*.npz")))]
 
 

@@ -136,6 +136,31 @@ int fft3d_b200_wisdom_import(const char *path);
 /* Drop every remembered choice (plans created afterwards time their candidates again). */
 void fft3d_b200_wisdom_forget(void);
 
+/* ---------------------------------------------------------------- 4D lattices (L^3 x T)
+ *
+ * The 4D DFT over (t, x, y, z) of `desc->batch` lattices of nt x n0 x n1 x n2
+ * points, element (b, t, x, y, z) at (((b*nt + t)*n0 + x)*n1 + y)*n2 + z: the
+ * asymmetric L^3 x T extents the reference names as the lattice-QCD target
+ * (docs/EXTENSIONS.md:55-64) and has no kernel for.  desc->n0..n2, direction,
+ * precision, flags and device are those of the 3D part; the inverse is scaled by
+ * 1/(nt*n0*n1*n2).  Supported: any 3D geometry this build has and
+ * nt in {2, 4, 6, 8, 12, 16, 17, 24, 32, 36, 48, 64}.  No counterpart exists in
+ * the reference. */
+
+typedef struct fft3d_b200_plan4d fft3d_b200_plan4d;
+
+/* Nonzero when nt x n0 x n1 x n2 lattices are supported in this precision. */
+int fft3d_b200_plan4d_supports(int nt, int n0, int n1, int n2, int precision);
+
+int fft3d_b200_plan4d_create(int nt, const fft3d_b200_desc *desc, fft3d_b200_plan4d **out);
+
+/* Device pointers, distinct buffers of batch*nt*n0*n1*n2 elements; asynchronous. */
+int fft3d_b200_plan4d_execute(fft3d_b200_plan4d *plan, const void *d_in, void *d_out, void *stream);
+
+void fft3d_b200_plan4d_destroy(fft3d_b200_plan4d *plan);
+
+const char *fft3d_b200_plan4d_describe(const fft3d_b200_plan4d *plan);
+
 /* ---------------------------------------------------------------- batches of uneven geometry */
 
 typedef struct {

@@ -415,6 +415,38 @@ extern "C" int hostcheck_mgpu(int L, int n, int sign, const void *in, void *out,
     return -2;
 }
 
+// The t pass of a 4D plan (plan4d.cu k_tpass) on the host: each spatial point
+// of each lattice, its nt points strided by V, in place.
+template <int TL, int SGN>
+static void emulate_tpass(cx<double> *data, long long vol_elems, long long batch)
+{
+    const double scale = SGN > 0 ? 1.0 / TL : 1.0;
+    for (long long b = 0; b < batch; ++b)
+        for (long long p = 0; p < vol_elems; ++p) {
+            cx<double> *col = data + b * TL * vol_elems + p;
+            cx<double> v[TL];
+            for (int t = 0; t < TL; ++t) v[t] = col[t * vol_elems];
+            dft<TL, SGN, double>(v);
+            for (int t = 0; t < TL; ++t) col[t * vol_elems] = SGN > 0 ? cscale(v[t], scale) : v[t];
+        }
+}
+
+extern "C" int hostcheck_tpass(int tl, int sign, void *data, long long vol_elems, long long batch)
+{
+    ensure_host_tables();
+    cx<double> *d = (cx<double> *)data;
+#define HC_TP(TL)                                                                   \
+    if (tl == TL) {                                                                 \
+        if (sign < 0) emulate_tpass<TL, -1>(d, vol_elems, batch);                   \
+        else emulate_tpass<TL, +1>(d, vol_elems, batch);                            \
+        return 0;                                                                   \
+    }
+    HC_TP(2) HC_TP(4) HC_TP(6) HC_TP(8) HC_TP(12) HC_TP(16) HC_TP(17) HC_TP(24) HC_TP(32)
+    HC_TP(36) HC_TP(48) HC_TP(64)
+#undef HC_TP
+    return -2;
+}
+
 // Items whose dependency wait would not hold when taken in ticket order (the
 // TWOPASS deadlock-freedom argument); reset by reading.
 extern "C" long long hostcheck_twopass_violations()

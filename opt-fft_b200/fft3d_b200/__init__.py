@@ -93,6 +93,9 @@ EXPORTS = {
                      "fft3d_b200_plan_launches", "fft3d_b200_last_status",
                      "fft3d_b200_status_string", "fft3d_b200_wisdom_export",
                      "fft3d_b200_wisdom_import", "fft3d_b200_wisdom_forget",
+                     "fft3d_b200_plan4d_supports", "fft3d_b200_plan4d_create",
+                     "fft3d_b200_plan4d_execute", "fft3d_b200_plan4d_destroy",
+                     "fft3d_b200_plan4d_describe",
                      "fft3d_b200_batch_create",
                      "fft3d_b200_batch_execute", "fft3d_b200_batch_destroy",
                      "fft3d_b200_batch_describe", "fft3d_b200_batch_execute_noalloc",
@@ -150,6 +153,11 @@ def _load():
         "fft3d_b200_wisdom_export": ([ctypes.c_char_p], i),
         "fft3d_b200_wisdom_import": ([ctypes.c_char_p], i),
         "fft3d_b200_wisdom_forget": ([], None),
+        "fft3d_b200_plan4d_supports": ([i, i, i, i, i], i),
+        "fft3d_b200_plan4d_create": ([i, ctypes.POINTER(Desc), ctypes.POINTER(vp)], i),
+        "fft3d_b200_plan4d_execute": ([vp, vp, vp, vp], i),
+        "fft3d_b200_plan4d_destroy": ([vp], None),
+        "fft3d_b200_plan4d_describe": ([vp], ctypes.c_char_p),
         "fft3d_b200_batch_create": ([ctypes.POINTER(Segment), i, ctypes.c_uint, i,
                                      ctypes.POINTER(vp)], i),
         "fft3d_b200_batch_execute": ([vp, vp], i),
@@ -219,6 +227,37 @@ def wisdom_import(path) -> int:
 def wisdom_forget():
     """Forget every autotuner choice of this process."""
     _lib.fft3d_b200_wisdom_forget()
+
+
+class Plan4D:
+    """4D DFT over (t, x, y, z) of `batch` lattices of nt x n0 x n1 x n2 (device
+    pointers): the tuned 3D plan over every time slice, then the t pass."""
+
+    def __init__(self, nt: int, shape, batch: int, direction: int = FORWARD,
+                 precision: int = C128, device: int = -1):
+        n0, n1, n2 = shape
+        self.nt, self.shape, self.batch = nt, tuple(shape), batch
+        d = Desc(n0, n1, n2, batch, direction, precision, 0, device)
+        h = ctypes.c_void_p()
+        _check(_lib.fft3d_b200_plan4d_create(nt, ctypes.byref(d), ctypes.byref(h)), "plan4d_create")
+        self._h = h
+
+    def execute(self, d_in: int, d_out: int, stream: int = 0):
+        _check(_lib.fft3d_b200_plan4d_execute(self._h, d_in, d_out, stream or None), "plan4d_execute")
+
+    def describe(self) -> str:
+        return _lib.fft3d_b200_plan4d_describe(self._h).decode()
+
+    def close(self):
+        if self._h:
+            _lib.fft3d_b200_plan4d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class MgpuPlan:

@@ -101,6 +101,14 @@ int fft3d_b200_plan_create_variant(const fft3d_b200_desc *desc, const char *vari
  * since the last check (FFT3D_B200_ERR_TIMEOUT when a bounded wait ran out). */
 int fft3d_b200_plan_check(fft3d_b200_plan *plan);
 
+/* Test hook, no counterpart in the reference: make the next device-pointer
+ * execute of a plan whose kernel keeps a scratch ring (TWOPASS variants) skip
+ * the first volume's plane items, so its dependent waits run out.  The launch
+ * ends by itself after the bounded wait (about 2 s), fft3d_b200_plan_check then
+ * reports FFT3D_B200_ERR_TIMEOUT, and later executes run normally.  Returns
+ * FFT3D_B200_ERR_UNSUPPORTED for other kernels. */
+int fft3d_b200_debug_stall_next_execute(fft3d_b200_plan *plan);
+
 /* Human-readable description of the kernel configuration the plan selected. */
 const char *fft3d_b200_plan_describe(const fft3d_b200_plan *plan);
 

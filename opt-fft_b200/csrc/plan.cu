@@ -675,6 +675,33 @@ extern "C" int fft3d_b200_plan_check(fft3d_b200_plan *p)
     return set_status(st);
 }
 
+// Test hook: start the next device-pointer execute of a TWOPASS plan at the
+// first row item's ticket.  The plane items of volume 0 are then never handed
+// out, so the row items that depend on them -- and, through the abort flag,
+// every other CTA -- give up after their bounded wait: the launch ends by
+// itself, fft3d_b200_plan_check reports FFT3D_B200_ERR_TIMEOUT, and the last
+// CTA leaves the control block cleared for the following execute.
+extern "C" int fft3d_b200_debug_stall_next_execute(fft3d_b200_plan *p)
+{
+    if (!p) return set_status(FFT3D_B200_ERR_INVALID);
+    if (p->kernel->family != FAM_TWOPASS || !p->work[0] || p->desc.batch < 1)
+        return set_status(FFT3D_B200_ERR_UNSUPPORTED);
+    const KernelEntry &e = *p->kernel;
+    const long long na = e.n0 / e.vpc, nb = e.n1 / e.vpc;
+    const long long grid = std::max(1LL, std::min((na + nb) * p->desc.batch, (long long)p->grid_limit));
+    int lag = 0;
+    twopass_ring(e, grid, &lag);
+    const long long nvol = p->desc.batch;
+    const unsigned long long first_row = nvol <= lag ? (unsigned long long)(na * nvol)
+                                                     : (unsigned long long)(na * lag + na);
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != p->device) cudaSetDevice(p->device);
+    const cudaError_t ce = cudaMemcpy(p->work[0], &first_row, sizeof first_row, cudaMemcpyHostToDevice);
+    if (prev >= 0 && prev != p->device) cudaSetDevice(prev);
+    return set_status(ce == cudaSuccess ? FFT3D_B200_OK : FFT3D_B200_ERR_CUDA);
+}
+
 extern "C" void fft3d_b200_plan_destroy(fft3d_b200_plan *p)
 {
     if (!p) return;

@@ -89,7 +89,7 @@ EXPORTS = {
                      "fft3d_b200_variants", "fft3d_b200_plan_create_variant",
                      "fft3d_b200_execute", "fft3d_b200_execute_host",
                      "fft3d_b200_execute_host_chain", "fft3d_b200_plan_describe",
-                     "fft3d_b200_plan_check",
+                     "fft3d_b200_plan_check", "fft3d_b200_debug_stall_next_execute",
                      "fft3d_b200_plan_launches", "fft3d_b200_last_status",
                      "fft3d_b200_status_string", "fft3d_b200_wisdom_export",
                      "fft3d_b200_wisdom_import", "fft3d_b200_wisdom_forget",
@@ -147,6 +147,7 @@ def _load():
         "fft3d_b200_execute_host_chain": ([ctypes.POINTER(vp), i, vp, vp], i),
         "fft3d_b200_plan_describe": ([vp], ctypes.c_char_p),
         "fft3d_b200_plan_check": ([vp], i),
+        "fft3d_b200_debug_stall_next_execute": ([vp], i),
         "fft3d_b200_plan_launches": ([vp], i),
         "fft3d_b200_last_status": ([], i),
         "fft3d_b200_status_string": ([i], ctypes.c_char_p),

@@ -12,8 +12,11 @@
  * owns the point's y range (peer stores: the all-to-all is fused into the
  * kernel), then each GPU transforms x over its y-slab.  execute() is
  * asynchronous and idempotent (it reads the uploaded input and writes the plan's
- * output buffers); download() waits for it.  Supported: L in {36, 45, 64} with
- * L divisible by ngpus, ngpus <= 16; the same device may appear more than once.
+ * output buffers); download() waits for it.  Supported: L in {36, 45, 64, 96,
+ * 128, 192, 256} with L divisible by ngpus, ngpus <= 16; the same device may
+ * appear more than once.  For L >= 96 (lines spread over 8 or 16 lanes, planes
+ * larger than shared memory) the z pass runs first into a per-GPU buffer and the
+ * exchange is fused into the y pass instead.
  */
 #ifndef FFT3D_MGPU_API_H
 #define FFT3D_MGPU_API_H

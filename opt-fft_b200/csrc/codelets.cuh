@@ -101,6 +101,11 @@ constexpr int tw_off(int n) { return n * (n - 1) / 2; }   // N = 1..TW_MAXN, pac
 constexpr int TW_ENTRIES = tw_off(TW_MAXN + 1);            // 2080
 // Rader-17 kernel spectra: [sign index][16], sign index 0 = forward, 1 = backward.
 constexpr int RADER17_ENTRIES = 32;
+// Line lengths above TW_MAXN (lines spread over several lanes): one table per N
+// in global memory, read through the read-only cache (lane-dependent indices
+// would serialise on the constant cache).
+constexpr int twbig_off(int n) { return n == 96 ? 0 : n == 128 ? 96 : n == 192 ? 224 : n == 256 ? 416 : -1; }
+constexpr int TWBIG_ENTRIES = 672;
 
 }  // namespace fft3d
 
@@ -112,8 +117,14 @@ extern __constant__ float2 c_tw_f[fft3d::TW_ENTRIES];
 extern __constant__ double2 c_rader17_d[fft3d::RADER17_ENTRIES];
 extern __constant__ float2 c_rader17_f[fft3d::RADER17_ENTRIES];
 #endif
+#if defined(__CUDACC__)
+extern __device__ double2 g_twbig_d[fft3d::TWBIG_ENTRIES];
+extern __device__ float2 g_twbig_f[fft3d::TWBIG_ENTRIES];
+#endif
 extern double2 h_tw_d[fft3d::TW_ENTRIES];
 extern float2 h_tw_f[fft3d::TW_ENTRIES];
+extern double2 h_twbig_d[fft3d::TWBIG_ENTRIES];
+extern float2 h_twbig_f[fft3d::TWBIG_ENTRIES];
 extern double2 h_rader17_d[fft3d::RADER17_ENTRIES];
 extern float2 h_rader17_f[fft3d::RADER17_ENTRIES];
 
@@ -140,6 +151,14 @@ struct Tab<double> {
         return h_rader17_d[i];
 #endif
     }
+    FFT_HD static double2 twbig(int i)
+    {
+#if defined(__CUDA_ARCH__)
+        return __ldg(&g_twbig_d[i]);
+#else
+        return h_twbig_d[i];
+#endif
+    }
 };
 
 template <>
@@ -158,6 +177,14 @@ struct Tab<float> {
         return c_rader17_f[i];
 #else
         return h_rader17_f[i];
+#endif
+    }
+    FFT_HD static float2 twbig(int i)
+    {
+#if defined(__CUDA_ARCH__)
+        return __ldg(&g_twbig_f[i]);
+#else
+        return h_twbig_f[i];
 #endif
     }
 };
@@ -190,7 +217,9 @@ FFT_HD cx<T> ctwiddle(cx<T> a, int E)
     if (4 * e == N) return cmul_iS<S>(a);
     if (2 * e == N) return {-a.re, -a.im};
     if (4 * e == 3 * N) return cmul_iS<-S>(a);
-    const auto w = Tab<T>::tw(tw_off(N) + e);  // {cos, sin}(2*pi*e/N)
+    static_assert(N <= TW_MAXN || twbig_off(N) >= 0, "no twiddle table for this extent");
+    const auto w = N <= TW_MAXN ? Tab<T>::tw(tw_off(N) + e)        // {cos, sin}(2*pi*e/N)
+                                : Tab<T>::twbig(twbig_off(N) + e);
     const T c = w.x;
     const T s = (S > 0) ? w.y : -w.y;
     return {a.re * c - a.im * s, a.re * s + a.im * c};

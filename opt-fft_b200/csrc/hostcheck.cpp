@@ -398,6 +398,56 @@ static void emulate_mgpu(int n, const cx<double> *in, cx<double> *out, long long
                         res[ky / m.S][mgpu_yslab_offset(m, b, kx, ky % m.S, kz)];
 }
 
+// Large L (mgpu.cu k_mgl_*): z lines of the x-slab into tmp, y lines of tmp to
+// the middle buffer of each point's y owner, x lines of each y-slab; every line
+// through split_line_host, the host form of the kernels' lane exchange.
+template <int L, int SGN>
+static void emulate_mgpu_large(int n, const cx<double> *in, cx<double> *out, long long B)
+{
+    const MgpuShape m{L, n, L / n};
+    const size_t slab = (size_t)B * m.S * L * L;
+    std::vector<cx<double>> tmp(slab);
+    std::vector<std::vector<cx<double>>> mid(n, std::vector<cx<double>>(slab, cx<double>{-1e300, 1e300}));
+    std::vector<std::vector<cx<double>>> res(n, std::vector<cx<double>>(slab));
+    const double scale = SGN > 0 ? 1.0 / ((double)L * L * L) : 1.0;
+    for (int g = 0; g < n; ++g) {
+        for (long long p = 0; p < B * m.S; ++p) {
+            const long long b = p / m.S, x = g * m.S + p % m.S;
+            const cx<double> *src = in + (b * L + x) * (long long)L * L;
+            cx<double> *t = tmp.data() + p * L * L;
+            for (int e = 0; e < L * L; ++e) t[e] = src[e];
+            for (int r = 0; r < L; ++r)
+                split_line_host<L, SGN, double>([&](int k) { return t[r * L + k]; },
+                                                [&](int k, cx<double> v) { t[r * L + k] = v; });
+            for (int z = 0; z < L; ++z)
+                split_line_host<L, SGN, double>([&](int y) { return t[y * L + z]; },
+                                                [&](int y, cx<double> v) { t[y * L + z] = v; });
+            for (int e = 0; e < L * L; ++e) {
+                int h;
+                const long long off = mgpu_mid_offset(m, g, p, e / L, e % L, &h);
+                mid[h][off] = t[e];
+            }
+        }
+    }
+    for (int h = 0; h < n; ++h)
+        for (long long r = 0; r < B * m.S; ++r) {
+            const long long b = r / m.S;
+            const int yl = (int)(r % m.S);
+            for (int z = 0; z < L; ++z)
+                split_line_host<L, SGN, double>(
+                    [&](int x) { return mid[h][mgpu_yslab_offset(m, b, x, yl, z)]; },
+                    [&](int x, cx<double> v) {
+                        res[h][mgpu_yslab_offset(m, b, x, yl, z)] = SGN > 0 ? cscale(v, scale) : v;
+                    });
+        }
+    for (long long b = 0; b < B; ++b)
+        for (int kx = 0; kx < L; ++kx)
+            for (int ky = 0; ky < L; ++ky)
+                for (int kz = 0; kz < L; ++kz)
+                    out[((b * L + kx) * L + ky) * (long long)L + kz] =
+                        res[ky / m.S][mgpu_yslab_offset(m, b, kx, ky % m.S, kz)];
+}
+
 extern "C" int hostcheck_mgpu(int L, int n, int sign, const void *in, void *out, long long B)
 {
     ensure_host_tables();
@@ -412,6 +462,14 @@ extern "C" int hostcheck_mgpu(int L, int n, int sign, const void *in, void *out,
     }
     HC_MG(36) HC_MG(45) HC_MG(64)
 #undef HC_MG
+#define HC_MGL(LL)                                                         \
+    if (L == LL) {                                                         \
+        if (sign < 0) emulate_mgpu_large<LL, -1>(n, x, y, B);              \
+        else emulate_mgpu_large<LL, +1>(n, x, y, B);                       \
+        return 0;                                                          \
+    }
+    HC_MGL(96) HC_MGL(128) HC_MGL(192) HC_MGL(256)
+#undef HC_MGL
     return -2;
 }
 

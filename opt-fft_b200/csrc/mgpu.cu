@@ -24,6 +24,7 @@
 #include "internal.h"
 #include "mgpu.cuh"
 #include "ptx.cuh"
+#include "splitline.cuh"
 
 namespace fft3d {
 
@@ -100,10 +101,124 @@ __global__ void __launch_bounds__(L < 64 ? 64 : L, 2)
     }
 }
 
+// ---------------------------------------------------------------- L = 96 .. 256
+// Lines too long for one thread and planes too large for shared memory: three
+// tiled passes, each line spread over P lanes (splitline.cuh), 128 threads and
+// C = 128 / P lines per tile.
+//   k_mgl_z  GPU g: C consecutive rows (z lines) of its x-slab, in -> tmp;
+//   k_mgl_y  GPU g: the y lines of C consecutive z of one plane, tmp -> the
+//            middle buffer of each point's y owner (the fused all-to-all);
+//   k_mgl_x  GPU h: the x lines of C consecutive z of one (volume, y) row of
+//            its y-slab, middle -> out.
+constexpr int MGL_THREADS = 128;
+
+template <int L>
+struct MglTile {
+    static constexpr int P = LineSplit<L>::P;
+    static constexpr int C = MGL_THREADS / P;  // lines per tile
+    static constexpr int CP = C + 1;           // padded row of a column tile
+    static constexpr int ZSMEM = C * L * (int)sizeof(cx<double>);
+    static constexpr int CSMEM = L * CP * (int)sizeof(cx<double>);
+    static_assert(L % C == 0, "tiles");
+};
+
+template <int L, int S>
+__global__ void __launch_bounds__(MGL_THREADS, 4)
+    k_mgl_z(const cx<double> *__restrict__ in, cx<double> *__restrict__ tmp, long long nrows)
+{
+    using TL = MglTile<L>;
+    constexpr int P = TL::P, C = TL::C;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cx<double> *sm = reinterpret_cast<cx<double> *>(smraw);
+    const int tid = threadIdx.x, c = tid / P, t = tid % P;
+    for (long long r0 = (long long)blockIdx.x * C; r0 < nrows; r0 += (long long)gridDim.x * C) {
+        const cx<double> *src = in + r0 * L;
+        for (int e = tid; e < C * L; e += MGL_THREADS) cp_async_16(sm + e, src + e);
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncthreads();
+        cx<double> *line = sm + c * L;
+        split_line<L, S, double>(t, true, [&](int k) { return line[k]; },
+                                 [&](int k, cx<double> v) { line[k] = v; });
+        __syncthreads();
+        cx<double> *dst = tmp + r0 * L;
+        for (int e = tid; e < C * L; e += MGL_THREADS) dst[e] = sm[e];
+        __syncthreads();
+    }
+}
+
+template <int L, int S>
+__global__ void __launch_bounds__(MGL_THREADS, 4)
+    k_mgl_y(const cx<double> *__restrict__ tmp, long long nplanes, cx<double> *const *__restrict__ mids,
+            MgpuShape m, int g)
+{
+    using TL = MglTile<L>;
+    constexpr int P = TL::P, C = TL::C, CP = TL::CP;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cx<double> *sm = reinterpret_cast<cx<double> *>(smraw);
+    const int tid = threadIdx.x, c = tid / P, t = tid % P;
+    const long long ntiles = nplanes * (L / C);
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const long long p = tile / (L / C);
+        const int z0 = (int)(tile % (L / C)) * C;
+        const cx<double> *src = tmp + p * L * L + z0;
+        for (int e = tid; e < L * C; e += MGL_THREADS) cp_async_16(sm + (e / C) * CP + e % C, src + (e / C) * L + e % C);
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncthreads();
+        split_line<L, S, double>(t, true, [&](int y) { return sm[y * CP + c]; },
+                                 [&](int y, cx<double> v) { sm[y * CP + c] = v; });
+        __syncthreads();
+        for (int e = tid; e < L * C; e += MGL_THREADS) {
+            const int y = e / C, z = z0 + e % C;
+            int h;
+            const long long off = mgpu_mid_offset(m, g, p, y, z, &h);
+            mids[h][off] = sm[y * CP + e % C];
+        }
+        __syncthreads();
+    }
+}
+
+template <int L, int S>
+__global__ void __launch_bounds__(MGL_THREADS, 4)
+    k_mgl_x(const cx<double> *__restrict__ mid, cx<double> *__restrict__ out, long long nrows, MgpuShape m,
+            double scale)
+{
+    using TL = MglTile<L>;
+    constexpr int P = TL::P, C = TL::C, CP = TL::CP;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cx<double> *sm = reinterpret_cast<cx<double> *>(smraw);
+    const int tid = threadIdx.x, c = tid / P, t = tid % P;
+    const long long ntiles = nrows * (L / C);
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const long long r = tile / (L / C);  // (volume, y) row of the y-slab
+        const long long b = r / m.S;
+        const int yl = (int)(r % m.S);
+        const int z0 = (int)(tile % (L / C)) * C;
+        for (int e = tid; e < L * C; e += MGL_THREADS)
+            cp_async_16(sm + (e / C) * CP + e % C, mid + mgpu_yslab_offset(m, b, e / C, yl, z0 + e % C));
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncthreads();
+        split_line<L, S, double>(t, true, [&](int x) { return sm[x * CP + c]; },
+                                 [&](int x, cx<double> v) { sm[x * CP + c] = v; });
+        __syncthreads();
+        for (int e = tid; e < L * C; e += MGL_THREADS) {
+            cx<double> v = sm[(e / C) * CP + e % C];
+            if constexpr (S > 0) v = cscale(v, scale);
+            store_out(out + mgpu_yslab_offset(m, b, e / C, yl, z0 + e % C), v);
+        }
+        __syncthreads();
+    }
+}
+
 struct MgpuKernels {
     int L;
-    const void *yz[2], *x[2];  // [0] forward, [1] inverse
-    int smem;
+    const void *yz[2], *x[2];  // [0] forward, [1] inverse; large L: the y pass
+    const void *z[2];          // large L only: the z pass (null otherwise)
+    int smem;                  // plane kernels / column tiles
+    int zsmem;                 // large L: row tiles
+    int tile_lines;            // large L: lines per tile (0 otherwise)
     int threads;
 };
 
@@ -117,14 +232,39 @@ static MgpuKernels mgpu_kernels()
     k.yz[1] = (const void *)&k_mg_yz<L, double, +1>;
     k.x[0] = (const void *)&k_mg_x<L, double, -1>;
     k.x[1] = (const void *)&k_mg_x<L, double, +1>;
+    k.z[0] = k.z[1] = nullptr;
     k.smem = G::PV * G::EB;
+    k.zsmem = 0;
+    k.tile_lines = 0;
     k.threads = L < 64 ? 64 : L;
+    return k;
+}
+
+template <int L>
+static MgpuKernels mgpu_kernels_large()
+{
+    using TL = MglTile<L>;
+    MgpuKernels k;
+    k.L = L;
+    k.z[0] = (const void *)&k_mgl_z<L, -1>;
+    k.z[1] = (const void *)&k_mgl_z<L, +1>;
+    k.yz[0] = (const void *)&k_mgl_y<L, -1>;
+    k.yz[1] = (const void *)&k_mgl_y<L, +1>;
+    k.x[0] = (const void *)&k_mgl_x<L, -1>;
+    k.x[1] = (const void *)&k_mgl_x<L, +1>;
+    k.smem = TL::CSMEM;
+    k.zsmem = TL::ZSMEM;
+    k.tile_lines = TL::C;
+    k.threads = MGL_THREADS;
     return k;
 }
 
 static const MgpuKernels *mgpu_find(int L)
 {
-    static const MgpuKernels table[] = {mgpu_kernels<36>(), mgpu_kernels<45>(), mgpu_kernels<64>()};
+    static const MgpuKernels table[] = {mgpu_kernels<36>(),        mgpu_kernels<45>(),
+                                        mgpu_kernels<64>(),        mgpu_kernels_large<96>(),
+                                        mgpu_kernels_large<128>(), mgpu_kernels_large<192>(),
+                                        mgpu_kernels_large<256>()};
     for (const auto &k : table)
         if (k.L == L) return &k;
     return nullptr;
@@ -143,10 +283,11 @@ struct fft3d_mgpu_plan {
     cx<double> *in[MGPU_MAX] = {};
     cx<double> *mid[MGPU_MAX] = {};
     cx<double> *out[MGPU_MAX] = {};
+    cx<double> *tmp[MGPU_MAX] = {};    // large L: the z-transformed x-slab
     cx<double> **mids[MGPU_MAX] = {};  // per GPU: device array of the n middle buffers
     cudaStream_t st[MGPU_MAX] = {};
     cudaEvent_t ev_yz[MGPU_MAX] = {}, ev_x[MGPU_MAX] = {};
-    int grid_yz[MGPU_MAX], grid_x[MGPU_MAX];
+    int grid_yz[MGPU_MAX], grid_x[MGPU_MAX], grid_z[MGPU_MAX];
 };
 
 extern "C" const char *fft3d_mgpu_name(void) { return "b200_slab_p2p"; }
@@ -174,6 +315,7 @@ extern "C" void fft3d_mgpu_destroy(fft3d_mgpu_plan *p)
         if (p->in[g]) cudaFree(p->in[g]);
         if (p->mid[g]) cudaFree(p->mid[g]);
         if (p->out[g]) cudaFree(p->out[g]);
+        if (p->tmp[g]) cudaFree(p->tmp[g]);
         if (p->mids[g]) cudaFree(p->mids[g]);
         if (p->st[g]) cudaStreamDestroy(p->st[g]);
         if (p->ev_yz[g]) cudaEventDestroy(p->ev_yz[g]);
@@ -226,6 +368,15 @@ extern "C" fft3d_mgpu_plan *fft3d_mgpu_create_ex(int L, int batch, int ngpus, co
              occ_yz > 0 && occ_x > 0;
         p->grid_yz[g] = occ_yz * sms;
         p->grid_x[g] = occ_x * sms;
+        p->grid_z[g] = 0;
+        if (ok && p->k->z[si]) {  // large L: the separate z pass and its buffer
+            int occ_z = 0;
+            ok = cudaMalloc(&p->tmp[g], bytes) == cudaSuccess &&
+                 cudaFuncSetAttribute(p->k->z[si], cudaFuncAttributeMaxDynamicSharedMemorySize, p->k->zsmem) == cudaSuccess &&
+                 cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_z, p->k->z[si], p->k->threads, p->k->zsmem) == cudaSuccess &&
+                 occ_z > 0;
+            p->grid_z[g] = occ_z * sms;
+        }
         // peer access to every other device of the list
         for (int h = 0; h < ngpus && ok; ++h) {
             if (devices[h] == devices[g]) continue;
@@ -286,11 +437,23 @@ extern "C" void fft3d_mgpu_execute(fft3d_mgpu_plan *p)
         cudaSetDevice(p->dev[g]);
         for (int h = 0; h < p->n; ++h) cudaStreamWaitEvent(p->st[g], p->ev_x[h], 0);
         const cx<double> *in = p->in[g];
+        long long yz_items = nplanes;
+        if (p->k->z[si]) {
+            // large L: z pass into tmp, then the y pass reads tmp
+            const long long nrows = nplanes * p->L;
+            const long long c = p->k->tile_lines;
+            cx<double> *tmp = p->tmp[g];
+            void *zargs[] = {(void *)&in, (void *)&tmp, (void *)&nrows};
+            const unsigned zgrid = (unsigned)std::min<long long>(nrows / c, p->grid_z[g]);
+            cudaLaunchKernel(p->k->z[si], dim3(zgrid), dim3(p->k->threads), zargs, (size_t)p->k->zsmem, p->st[g]);
+            in = tmp;
+            yz_items = nplanes * (p->L / c);
+        }
         cx<double> *const *mids = p->mids[g];
         MgpuShape m = p->m;
         int gg = g;
         void *args[] = {(void *)&in, (void *)&nplanes, (void *)&mids, (void *)&m, (void *)&gg};
-        const unsigned grid = (unsigned)std::min<long long>(nplanes, p->grid_yz[g]);
+        const unsigned grid = (unsigned)std::min<long long>(yz_items, p->grid_yz[g]);
         cudaLaunchKernel(p->k->yz[si], dim3(grid), dim3(p->k->threads), args, (size_t)p->k->smem, p->st[g]);
         cudaEventRecord(p->ev_yz[g], p->st[g]);
     }
@@ -302,7 +465,8 @@ extern "C" void fft3d_mgpu_execute(fft3d_mgpu_plan *p)
         MgpuShape m = p->m;
         double sc = scale;
         void *args[] = {(void *)&mid, (void *)&out, (void *)&nplanes, (void *)&m, (void *)&sc};
-        const unsigned grid = (unsigned)std::min<long long>(nplanes, p->grid_x[h]);
+        const long long x_items = p->k->tile_lines ? nplanes * (p->L / p->k->tile_lines) : nplanes;
+        const unsigned grid = (unsigned)std::min<long long>(x_items, p->grid_x[h]);
         cudaLaunchKernel(p->k->x[si], dim3(grid), dim3(p->k->threads), args, (size_t)p->k->smem, p->st[h]);
         cudaEventRecord(p->ev_x[h], p->st[h]);
     }

@@ -36,6 +36,27 @@ struct LineSplit<64> {
     static constexpr int P = 4, Q = 16;
     static constexpr bool PFA = false;
 };
+// Lines longer than one thread can hold (the multi-GPU large cubes).
+template <>
+struct LineSplit<96> {
+    static constexpr int P = 8, Q = 12;
+    static constexpr bool PFA = false;
+};
+template <>
+struct LineSplit<128> {
+    static constexpr int P = 8, Q = 16;
+    static constexpr bool PFA = false;
+};
+template <>
+struct LineSplit<192> {
+    static constexpr int P = 16, Q = 12;
+    static constexpr bool PFA = false;
+};
+template <>
+struct LineSplit<256> {
+    static constexpr int P = 16, Q = 16;
+    static constexpr bool PFA = false;
+};
 
 template <int N>
 struct SplitMap {

@@ -8,6 +8,8 @@ __constant__ double2 c_tw_d[fft3d::TW_ENTRIES];
 __constant__ float2 c_tw_f[fft3d::TW_ENTRIES];
 __constant__ double2 c_rader17_d[fft3d::RADER17_ENTRIES];
 __constant__ float2 c_rader17_f[fft3d::RADER17_ENTRIES];
+__device__ double2 g_twbig_d[fft3d::TWBIG_ENTRIES];
+__device__ float2 g_twbig_f[fft3d::TWBIG_ENTRIES];
 
 namespace fft3d {
 
@@ -25,6 +27,9 @@ int ensure_device_tables(int device)
     if (cudaMemcpyToSymbol(c_rader17_d, h_rader17_d, sizeof(h_rader17_d)) != cudaSuccess)
         return FFT3D_B200_ERR_CUDA;
     if (cudaMemcpyToSymbol(c_rader17_f, h_rader17_f, sizeof(h_rader17_f)) != cudaSuccess)
+        return FFT3D_B200_ERR_CUDA;
+    if (cudaMemcpyToSymbol(g_twbig_d, h_twbig_d, sizeof(h_twbig_d)) != cudaSuccess ||
+        cudaMemcpyToSymbol(g_twbig_f, h_twbig_f, sizeof(h_twbig_f)) != cudaSuccess)
         return FFT3D_B200_ERR_CUDA;
     if (tc_tables_upload() != FFT3D_B200_OK) return FFT3D_B200_ERR_CUDA;
     g_dev_done[device] = true;

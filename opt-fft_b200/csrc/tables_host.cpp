@@ -16,6 +16,8 @@ double2 h_tw_d[fft3d::TW_ENTRIES];
 float2 h_tw_f[fft3d::TW_ENTRIES];
 double2 h_rader17_d[fft3d::RADER17_ENTRIES];
 float2 h_rader17_f[fft3d::RADER17_ENTRIES];
+double2 h_twbig_d[fft3d::TWBIG_ENTRIES];
+float2 h_twbig_f[fft3d::TWBIG_ENTRIES];
 
 namespace fft3d {
 
@@ -45,6 +47,14 @@ static void fill_host_tables()
             exact_cis(e, n, &c, &s);
             h_tw_d[tw_off(n) + e] = make_double2((double)c, (double)s);
             h_tw_f[tw_off(n) + e] = make_float2((float)c, (float)s);
+        }
+    }
+    for (int n : {96, 128, 192, 256}) {
+        for (int e = 0; e < n; ++e) {
+            long double c, s;
+            exact_cis(e, n, &c, &s);
+            h_twbig_d[twbig_off(n) + e] = make_double2((double)c, (double)s);
+            h_twbig_f[twbig_off(n) + e] = make_float2((float)c, (float)s);
         }
     }
     // Rader-17 kernel spectra for both exponent signs.

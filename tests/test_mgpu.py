@@ -23,14 +23,15 @@ import fft3d_b200 as fb
 
 C128_TOL = 1e-13
 CPU_CASES = [(36, 1), (36, 2), (36, 3), (36, 4), (36, 6), (36, 9), (36, 12), (45, 3), (45, 5),
-             (45, 9), (64, 1), (64, 2), (64, 4), (64, 8), (64, 16)]
+             (45, 9), (64, 1), (64, 2), (64, 4), (64, 8), (64, 16), (96, 1), (96, 3), (128, 2),
+             (128, 8), (192, 4), (256, 2)]
 
 
 @pytest.mark.parametrize("L,n", CPU_CASES, ids=[f"L{c[0]}-n{c[1]}" for c in CPU_CASES])
 @pytest.mark.parametrize("sign", [-1, +1])
 def test_slab_exchange_on_cpu(hostcheck, L, n, sign):
     hostcheck.hostcheck_mgpu.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p] * 2 + [ctypes.c_longlong]
-    B = 2
+    B = 2 if L <= 64 else 1
     rng = np.random.default_rng(L * 31 + n)
     x = field(rng, (B, L, L, L), dist="normal")
     out = np.empty_like(x)
@@ -44,13 +45,13 @@ def test_supports_matrix():
     assert lib.fft3d_mgpu_name() == b"b200_slab_p2p"
     for L, n in CPU_CASES:
         assert lib.fft3d_mgpu_supports(L, n) == 1
-    for L, n in ((64, 3), (36, 5), (96, 2), (128, 8), (256, 8), (64, 0), (64, 32)):
+    for L, n in ((64, 3), (36, 5), (96, 5), (128, 3), (256, 3), (64, 0), (64, 32), (100, 2)):
         assert lib.fft3d_mgpu_supports(L, n) == 0
 
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("L,n,B", [(64, 1, 2), (64, 2, 3), (64, 4, 1), (36, 3, 4), (45, 5, 2),
-                                   (36, 12, 2)])
+                                   (36, 12, 2), (96, 2, 2), (128, 4, 1), (192, 3, 1), (256, 2, 1)])
 def test_mgpu_matches_oracle(L, n, B):
     rng = np.random.default_rng(L + 7 * n + B)
     x = field(rng, (B, L, L, L))
@@ -91,5 +92,5 @@ def test_mgpu_create_refuses_bad_arguments():
     lib = fb.lib()
     devs = (ctypes.c_int * 2)(0, 99)
     assert not lib.fft3d_mgpu_create(64, 1, 2, devs)         # no such device
-    assert not lib.fft3d_mgpu_create(96, 1, 2, (ctypes.c_int * 2)(0, 0))  # unsupported L
+    assert not lib.fft3d_mgpu_create(100, 1, 2, (ctypes.c_int * 2)(0, 0))  # unsupported L
     assert not lib.fft3d_mgpu_create(64, 0, 1, (ctypes.c_int * 1)(0))     # empty batch

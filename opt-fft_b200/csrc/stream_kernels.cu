@@ -202,6 +202,8 @@ void register_stream_kernels(std::vector<KernelEntry> &out)
     FFT3D_STREAM(8, 8, 8, double, 0, 4, 256, 4, 1);
     FFT3D_STREAM(8, 8, 8, double, 0, 2, 128, 3, 2);
     FFT3D_STREAM(8, 8, 8, double, 0, 8, 512, 2, 1);
+    FFT3D_STREAM(8, 8, 8, double, 0, 1, 64, 3, 8);   // one volume per item: even tails
+    FFT3D_STREAM(8, 8, 8, double, 0, 1, 64, 4, 6);
     FFT3D_STREAM(12, 12, 12, double, 0, 2, 288, 2, 1);
     FFT3D_STREAM(12, 12, 12, double, 0, 1, 160, 3, 2);
     FFT3D_STREAM(16, 16, 16, double, 0, 1, 256, 2, 1);

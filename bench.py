@@ -38,8 +38,9 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 L2_BYTES = 126 * 1024 * 1024
 # how the device-timed region was launched (filled in by time_device)
-TIMING = {"launch": "timed steps captured in one CUDA graph, replayed once between two events; "
-                    "per-launch times from event record nodes", "graph_uploaded": None}
+TIMING = {"launch": "timed steps captured in one CUDA graph of launches only, replayed once "
+                    "between two events; per-launch time = graph time / launches",
+          "graph_uploaded": None}
 
 WORKLOADS = {
     "roundtrip17": dict(shape=(17, 17, 17), batch=2048, prec=0, chain=(-1, +1), dist="uniform",
@@ -186,15 +187,11 @@ class Workload:
         self.tdt = tdt
         self.it = 0
 
-    def step(self, stream, ev=None):
+    def step(self, stream):
         bufs = self.sets[self.it % self.nsets]
         self.it += 1
         for k, p in enumerate(self.plans):
-            if ev is not None and k == 0:
-                ev[0].record(stream)
             p.execute(bufs[k].data_ptr(), bufs[k + 1].data_ptr(), stream.cuda_stream)
-            if ev is not None and k == 0:
-                ev[1].record(stream)
 
     def launches_per_step(self):
         return sum(p.launches() for p in self.plans)
@@ -210,14 +207,13 @@ class CopyFloor:
         self.wl = wl
         self.it = 0
 
-    def step(self, stream, ev=None):
+    def step(self, stream):
         bufs = self.wl.sets[self.it % self.wl.nsets]
         self.it += 1
-        if ev is not None:
-            ev[0].record(stream)
         bufs[1].copy_(bufs[0])
-        if ev is not None:
-            ev[1].record(stream)
+
+    def launches_per_step(self):
+        return 1
 
 
 def copy_floor(torch, wl, stream, steps, warmup):
@@ -244,17 +240,17 @@ def time_device(torch, wl, stream, steps, warmup, dist=None, sampler=None):
     steps captured into one CUDA graph (the launch path a serving loop uses),
     uploaded, and replayed once between two events.  Without the graph a
     kernel of ~15 us waits on the Python loop that enqueues it, and that host
-    time would be charged to the kernel.  Per-launch durations come from event
-    record nodes around the first launch of every step."""
+    time would be charged to the kernel.  The graph holds the launches only
+    (no event nodes between them, which would also cut the programmatic
+    dependent-launch edges), so the average launch duration is the graph's
+    time over its launches.  Returns (ms per step, ms per launch, clocks)."""
     for _ in range(warmup):
         wl.step(stream)
     torch.cuda.synchronize()
-    evs = [(torch.cuda.Event(enable_timing=True, external=True),
-            torch.cuda.Event(enable_timing=True, external=True)) for _ in range(steps)]
     graph = torch.cuda.CUDAGraph()
     with torch.cuda.graph(graph, stream=stream):
         for k in range(steps):
-            wl.step(stream, evs[k])
+            wl.step(stream)
     uploaded = _graph_upload(torch, graph, stream)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -271,14 +267,13 @@ def time_device(torch, wl, stream, steps, warmup, dist=None, sampler=None):
     clocks = sampler.stop() if sampler else None
     TIMING["graph_uploaded"] = uploaded
     total_ms = e0.elapsed_time(e1)
-    first_ms = [a.elapsed_time(b) for a, b in evs]
     del graph
     if dist is not None:
         t = torch.tensor([total_ms], dtype=torch.float64, device=stream.device)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
         dist.barrier()
-    return total_ms / steps, statistics.mean(first_ms), clocks
+    return total_ms / steps, total_ms / (steps * wl.launches_per_step()), clocks
 
 
 def time_e2e(fb, torch, wl, steps, warmup, dist=None):
@@ -656,16 +651,16 @@ def main():
 
     wl = Workload(fb, torch, a.workload, device, seed=1234 + rank, variant=a.variant)
     sampler = ClockSampler(local)
-    ms, first_ms, clocks = time_device(torch, wl, stream, a.steps, a.warmup, dist, sampler)
+    ms, per_launch_ms, clocks = time_device(torch, wl, stream, a.steps, a.warmup, dist, sampler)
     value = world * wl.batch / (ms * 1e-3)
     alg_bytes = 2 * wl.bytes
-    achieved = alg_bytes / (first_ms * 1e-3) / 1e9
+    achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
                 "kernel": wl.plans[0].describe(),
                 "alg_bytes_per_launch": alg_bytes,
                 "traffic": traffic.get(a.workload.replace("roundtrip", "fwd")),
-                "ms_per_launch": first_ms}
+                "ms_per_launch": per_launch_ms}
     cf = copy_floor(torch, wl, stream, min(a.steps, 200), a.warmup)
     roofline["copy_same_bytes_gbs"] = cf
     roofline["frac_of_copy_same_bytes"] = achieved / cf

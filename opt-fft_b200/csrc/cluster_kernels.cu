@@ -45,6 +45,7 @@ __global__ void __launch_bounds__(NT, 1)
     constexpr int PL = CL::PL;
     constexpr int V = N0 * N1 * N2;
     static_assert(N0 % C == 0 && (N1 * N2) % C == 0, "cluster split");
+    pdl_begin();
     extern __shared__ __align__(128) unsigned char smraw[];
     cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);
     uint64_t *xbar = reinterpret_cast<uint64_t *>(smraw + CL::SLAB_BYTES);

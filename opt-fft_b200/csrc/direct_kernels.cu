@@ -8,6 +8,7 @@
 // copies (stage in, z, y, x) to four, and there is no staging copy to wait for:
 // latency is hidden by running several small CTAs per SM.
 #include "internal.h"
+#include "ptx.cuh"
 #include "volume.cuh"
 
 namespace fft3d {
@@ -17,6 +18,7 @@ __global__ void __launch_bounds__(NT, MINB)
     k_direct(const cx<typename G::T> *__restrict__ in, cx<typename G::T> *__restrict__ out,
              long long nvol, typename G::T scale)
 {
+    pdl_begin();
     using T = typename G::T;
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);

@@ -296,7 +296,7 @@ static const EmuEntry kEmu[] = {
     EMU_BIG(36, double, 9),        EMU_BIG(36, float, 12),
     EMU_TP(36, 36, 36, double, 4), EMU_TP(36, 36, 36, double, 2),  EMU_TP(36, 36, 36, double, 6),
     EMU_TP(36, 36, 36, float, 4),  EMU_TP(36, 36, 36, float, 6),   EMU_TP(16, 16, 32, double, 4),
-    EMU_TP(16, 16, 32, double, 8), EMU_TP(6, 9, 5, double, 3),
+    EMU_TP(16, 16, 32, double, 8), EMU_TP(6, 9, 5, double, 3),     EMU_TP(36, 36, 36, double, 3),
     EMU(13, 13, 13, double, 0, 2), EMU(23, 23, 23, double, 0, 1),  EMU(13, 13, 13, float, 0, 4),
     EMU(23, 23, 23, float, 0, 1),  EMU_TP(45, 45, 45, double, 3), EMU_TP(45, 45, 45, float, 5),
     EMU_TP(64, 64, 64, double, 1), EMU_TP(64, 64, 64, float, 2),

@@ -52,6 +52,47 @@ const std::vector<KernelEntry> &registry()
     return reg;
 }
 
+// Programmatic dependent launch for every kernel started here (each calls
+// pdl_begin() before touching global memory): the CTAs of a launch are placed
+// while the previous kernel of the stream drains, and start work the moment it
+// completes.  FFT3D_B200_PDL=0 turns it off (plain stream order); the legacy
+// default stream always gets plain order.
+static bool pdl_enabled()
+{
+    static const bool on = [] {
+        const char *v = std::getenv("FFT3D_B200_PDL");
+        return !(v && v[0] == '0');
+    }();
+    return on;
+}
+
+static cudaError_t launch_ex(const KernelEntry &e, dim3 grid, void **args, cudaStream_t stream,
+                             unsigned cluster /* CTAs per cluster, 0: none */)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(e.threads);
+    cfg.dynamicSmemBytes = (size_t)e.smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[2];
+    unsigned n = 0;
+    if (cluster) {
+        attr[n].id = cudaLaunchAttributeClusterDimension;
+        attr[n].val.clusterDim.x = cluster;
+        attr[n].val.clusterDim.y = 1;
+        attr[n].val.clusterDim.z = 1;
+        ++n;
+    }
+    if (pdl_enabled() && stream != nullptr && stream != cudaStreamLegacy) {
+        attr[n].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[n].val.programmaticStreamSerializationAllowed = 1;
+        ++n;
+    }
+    cfg.attrs = attr;
+    cfg.numAttrs = n;
+    return cudaLaunchKernelExC(&cfg, e.func, args);
+}
+
 cudaError_t launch_entry(const KernelEntry &e, const void *in, void *out, long long nvol,
                          double scale, cudaStream_t stream, int grid_limit, int *err, void *work)
 {
@@ -67,14 +108,12 @@ cudaError_t launch_entry(const KernelEntry &e, const void *in, void *out, long l
             double s = scale;
             void *args[] = {(void *)&in, (void *)&out, (void *)&nvol, (void *)&s,
                             (void *)&err, (void *)&w,  (void *)&ring, (void *)&lag};
-            return cudaLaunchKernel(e.func, dim3((unsigned)grid), dim3(e.threads), args,
-                                    (size_t)e.smem, stream);
+            return launch_ex(e, dim3((unsigned)grid), args, stream, 0);
         } else {
             float s = (float)scale;
             void *args[] = {(void *)&in, (void *)&out, (void *)&nvol, (void *)&s,
                             (void *)&err, (void *)&w,  (void *)&ring, (void *)&lag};
-            return cudaLaunchKernel(e.func, dim3((unsigned)grid), dim3(e.threads), args,
-                                    (size_t)e.smem, stream);
+            return launch_ex(e, dim3((unsigned)grid), args, stream, 0);
         }
     }
     if (e.family == FAM_STREAM) {
@@ -83,13 +122,11 @@ cudaError_t launch_entry(const KernelEntry &e, const void *in, void *out, long l
         if (e.precision == FFT3D_B200_C128) {
             double s = scale;
             void *args[] = {(void *)&in, (void *)&out, (void *)&nvol, (void *)&s, (void *)&err};
-            return cudaLaunchKernel(e.func, dim3((unsigned)grid), dim3(e.threads), args,
-                                    (size_t)e.smem, stream);
+            return launch_ex(e, dim3((unsigned)grid), args, stream, 0);
         } else {
             float s = (float)scale;
             void *args[] = {(void *)&in, (void *)&out, (void *)&nvol, (void *)&s, (void *)&err};
-            return cudaLaunchKernel(e.func, dim3((unsigned)grid), dim3(e.threads), args,
-                                    (size_t)e.smem, stream);
+            return launch_ex(e, dim3((unsigned)grid), args, stream, 0);
         }
     }
     if (e.family == FAM_VOLUME) {
@@ -98,38 +135,25 @@ cudaError_t launch_entry(const KernelEntry &e, const void *in, void *out, long l
         if (e.precision == FFT3D_B200_C128) {
             double s = scale;
             void *args[] = {(void *)&in, (void *)&out, (void *)&nvol, (void *)&s};
-            return cudaLaunchKernel(e.func, dim3((unsigned)grid), dim3(e.threads), args,
-                                    (size_t)e.smem, stream);
+            return launch_ex(e, dim3((unsigned)grid), args, stream, 0);
         } else {
             float s = (float)scale;
             void *args[] = {(void *)&in, (void *)&out, (void *)&nvol, (void *)&s};
-            return cudaLaunchKernel(e.func, dim3((unsigned)grid), dim3(e.threads), args,
-                                    (size_t)e.smem, stream);
+            return launch_ex(e, dim3((unsigned)grid), args, stream, 0);
         }
     }
     if (e.family == FAM_CLUSTER) {
         // one cluster of e.vpc CTAs per volume
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3((unsigned)(nvol * e.vpc));
-        cfg.blockDim = dim3(e.threads);
-        cfg.dynamicSmemBytes = (size_t)e.smem;
-        cfg.stream = stream;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = e.vpc;
-        attr[0].val.clusterDim.y = 1;
-        attr[0].val.clusterDim.z = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
         if (nvol * e.vpc > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+        const dim3 grid((unsigned)(nvol * e.vpc));
         if (e.precision == FFT3D_B200_C128) {
             double s = scale;
             void *args[] = {(void *)&in, (void *)&out, (void *)&nvol, (void *)&s, (void *)&err};
-            return cudaLaunchKernelExC(&cfg, e.func, args);
+            return launch_ex(e, grid, args, stream, (unsigned)e.vpc);
         } else {
             float s = (float)scale;
             void *args[] = {(void *)&in, (void *)&out, (void *)&nvol, (void *)&s, (void *)&err};
-            return cudaLaunchKernelExC(&cfg, e.func, args);
+            return launch_ex(e, grid, args, stream, (unsigned)e.vpc);
         }
     }
     return cudaErrorInvalidValue;

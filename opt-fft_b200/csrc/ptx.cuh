@@ -236,4 +236,18 @@ __device__ __forceinline__ void report_error(int *err, int code)
     if (err) atomicCAS(err, 0, code);
 }
 
+// Programmatic dependent launch.  A kernel launched with the programmatic
+// stream-serialization attribute may have its CTAs placed while the previous
+// kernel of the stream drains; griddepcontrol.wait then blocks until that
+// kernel has completed and its memory operations are visible, so everything
+// after it may read the previous kernel's output and overwrite its input.
+// Without the attribute the wait returns at once.  launch_dependents lets the
+// next such kernel place its CTAs as ours exit.  Called first in every kernel
+// that launch_entry starts, before any global memory access.
+__device__ __forceinline__ void pdl_begin()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 }  // namespace fft3d

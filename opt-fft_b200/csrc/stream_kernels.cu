@@ -73,6 +73,7 @@ __global__ void __launch_bounds__(NT, MINB)
              long long nvol, typename G::T scale, int *err)
 {
     static_assert(NSTAGE >= 1 && NSTAGE <= 4, "ring depth");
+    pdl_begin();
     using T = typename G::T;
     using SL = StreamLayout<G, VPC, NSTAGE>;
     extern __shared__ __align__(128) unsigned char smraw[];

@@ -203,6 +203,7 @@ __global__ void __launch_bounds__(256, 1)
     k_tc(const cx<float> *__restrict__ in, cx<float> *__restrict__ out, long long nvol, float scale,
          int *err)
 {
+    pdl_begin();
     using C = TcCfg<L, VPC, SPLIT>;
     using G = typename C::G;
     // The dynamic segment follows the static one (s_abort) and starts only

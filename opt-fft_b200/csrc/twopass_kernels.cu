@@ -128,6 +128,7 @@ __global__ void __launch_bounds__(NT, MINB)
     k_twopass(const cx<T> *__restrict__ in, cx<T> *__restrict__ out, long long nvol, T scale,
               int *err, unsigned char *work, int R, int D)
 {
+    pdl_begin();
     using TG = TwoPassGeom<N0, N1, N2, T, G>;
     using XG = typename TG::XG;
     using YG = typename TG::YG;
@@ -321,6 +322,7 @@ __global__ void __launch_bounds__(NT, MINB)
     k_twopass_pipe(const cx<double> *__restrict__ in, cx<double> *__restrict__ out, long long nvol,
                    double scale, int *err, unsigned char *work, int R, int D)
 {
+    pdl_begin();
     using T = double;
     using TG = TwoPassGeom<N0, N1, N2, T, G>;
     using XG = typename TG::XG;
@@ -532,6 +534,7 @@ void register_twopass_kernels(std::vector<KernelEntry> &out)
 {
     // rows moved by bulk copies: almost no integer work outside the transform
     FFT3D_TWOPASS_BULK(36, 36, 36, 2, 96, 4);
+    FFT3D_TWOPASS_BULK(36, 36, 36, 3, 128, 3);  // 108 lines on 4 warps: 84% of lanes busy
     FFT3D_TWOPASS_BULK(36, 36, 36, 4, 160, 2);
     FFT3D_TWOPASS_BULK(36, 36, 36, 1, 64, 6);
     FFT3D_TWOPASS_BULK(45, 45, 45, 3, 160, 2);

@@ -8,6 +8,7 @@
 // row-column structure of python/fft3d.py:349-399 and of the fused A100 kernels of
 // the reference (bench/gpu/impl_4/L17_dmma.cu:36-38), laid out for sm_100a.
 #include "internal.h"
+#include "ptx.cuh"
 #include "volume.cuh"
 
 namespace fft3d {
@@ -17,6 +18,7 @@ __global__ void __launch_bounds__(NT, MINB)
     k_volume(const cx<typename G::T> *__restrict__ in, cx<typename G::T> *__restrict__ out,
              long long nvol, typename G::T scale)
 {
+    pdl_begin();
     using T = typename G::T;
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);

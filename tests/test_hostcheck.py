@@ -101,7 +101,8 @@ def test_two_phase_cube(hostcheck, prec, pl, sign):
 TWOPASS = [((36, 36, 36), 0, 4, 11), ((36, 36, 36), 0, 2, 3), ((36, 36, 36), 0, 6, 9),
            ((36, 36, 36), 1, 4, 11), ((36, 36, 36), 1, 6, 2), ((16, 16, 32), 0, 4, 13),
            ((16, 16, 32), 0, 8, 1), ((6, 9, 5), 0, 3, 41), ((45, 45, 45), 0, 3, 5),
-           ((45, 45, 45), 1, 5, 3), ((64, 64, 64), 0, 1, 3), ((64, 64, 64), 1, 2, 2)]
+           ((45, 45, 45), 1, 5, 3), ((64, 64, 64), 0, 1, 3), ((64, 64, 64), 1, 2, 2),
+           ((36, 36, 36), 0, 3, 7)]
 
 
 @pytest.mark.parametrize("shape,prec,g,nvol", TWOPASS,

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "mgpu.cuh"
+#include "pfa36.cuh"
 #include "splitline.cuh"
 #include "twopass.cuh"
 #include "volume.cuh"
@@ -174,6 +175,126 @@ static void emulate_twopass(const void *vin, void *vout, long long nvol)
     }
 }
 
+// The lean-control TWOPASS variants (k_twopass_regs): z pass in the plane
+// layout; y pass stored straight into the slot (YDIRECT) or in shared memory
+// and copied by rows; x pass loaded straight from the slot or from rows
+// gathered into the row layout (XBULK).  Same tickets, ring and dependency
+// checks as emulate_twopass.
+template <int N0, int N1, int N2, typename T, int S, int G, bool XBULK, bool YDIRECT>
+static void emulate_twopass_regs(const void *vin, void *vout, long long nvol)
+{
+    using TG = TwoPassGeom<N0, N1, N2, T, G>;
+    using XG = typename TG::XG;
+    using YG = typename TG::YG;
+    const T scale = S > 0 ? T(1) / T(TG::V) : T(1);
+    int lag = 0;
+    const int R = twopass_ring_size(TG::NA, TG::NB, 7, &lag);
+    std::vector<cx<T>> sm((size_t)TG::PV), ring((size_t)R * TG::V, cx<T>{T(-777.0), T(555.0)});
+    const cx<T> *in = (const cx<T> *)vin;
+    cx<T> *out = (cx<T> *)vout;
+    const long long total = (long long)(TG::NA + TG::NB) * nvol;
+    std::vector<long long> cnt_plane(R, 0), cnt_row(R, 0);
+    for (long long t = 0; t < total; ++t) {
+        const TwoPassItem it = twopass_decode(t, nvol, TG::NA, TG::NB, lag);
+        const int slot = (int)(it.vol % R);
+        const long long round = it.vol / R;
+        cx<T> *sv = ring.data() + slot * TG::V;
+        if (it.plane ? cnt_row[slot] < TG::NB * round : cnt_plane[slot] < TG::NA * (round + 1))
+            g_twopass_violations++;
+        (it.plane ? cnt_plane : cnt_row)[slot]++;
+        for (auto &e : sm) e = {T(12345.0), T(-6789.0)};
+        if (it.plane) {
+            const cx<T> *rows = in + it.vol * TG::V + (long long)it.j * G * N1 * N2;
+            for (int r = 0; r < XG::ROWS; ++r)  // the bulk copy of row r
+                for (int z = 0; z < N2; ++z) sm[XG::off(r, z)] = rows[(long long)r * N2 + z];
+            for (int r = 0; r < XG::ROWS; ++r) pass_z<XG, S, ALG_DEFAULT>(sm.data(), r);
+            if (YDIRECT) {
+                for (int l = 0; l < G * N2; ++l) pass_y_store_l2<XG, S>(sm.data(), l, sv, it.j * G);
+            } else {
+                for (int l = 0; l < G * N2; ++l) pass_y<XG, S, ALG_DEFAULT>(sm.data(), l);
+                cx<T> *dst = sv + (long long)it.j * G * N1 * N2;
+                for (int r = 0; r < XG::ROWS; ++r)
+                    for (int z = 0; z < N2; ++z) dst[(long long)r * N2 + z] = sm[XG::off(r, z)];
+            }
+        } else if (XBULK) {
+            for (int q = 0; q < N0 * G; ++q) {
+                const int x = q / G, yl = q % G;
+                for (int z = 0; z < N2; ++z)
+                    sm[YG::off(q, z)] = sv[((long long)x * N1 + it.j * G + yl) * N2 + z];
+            }
+            for (int l = 0; l < G * N2; ++l)
+                pass_x_slab<YG, S, N1>(sm.data(), l, out + it.vol * TG::V, it.j * G, scale);
+        } else {
+            for (int l = 0; l < G * N2; ++l)
+                pass_x_load_l2<N0, N1, N2, S, T>(sv, l, out + it.vol * TG::V, it.j * G, scale);
+        }
+    }
+}
+
+// The 36^3 TWOPASS variant with lines split into 4 x 9 stages
+// (k_twopass_pfa): every stage-1 task of a pass, then every stage-2 task, as
+// the kernel's barrier between them orders them; tickets, ring and dependency
+// checks as emulate_twopass.
+template <int S, int G>
+static void emulate_twopass_pfa(const void *vin, void *vout, long long nvol)
+{
+    constexpr int N = 36, LINES = G * N;
+    constexpr long long PLANE = (long long)N * N;
+    using T = double;
+    using TG = TwoPassGeom<N, N, N, T, G>;
+    using XG = typename TG::XG;
+    using YG = typename TG::YG;
+    const T scale = S > 0 ? T(1) / T(TG::V) : T(1);
+    int lag = 0;
+    const int R = twopass_ring_size(TG::NA, TG::NB, 7, &lag);
+    std::vector<cx<T>> smv((size_t)TG::PV), ring((size_t)R * TG::V, cx<T>{T(-777.0), T(555.0)});
+    cx<T> *sm = smv.data();
+    const cx<T> *in = (const cx<T> *)vin;
+    cx<T> *out = (cx<T> *)vout;
+    const long long total = (long long)(TG::NA + TG::NB) * nvol;
+    std::vector<long long> cnt_plane(R, 0), cnt_row(R, 0);
+    auto zaddr = [](int l, int e) { return XG::off(l, e); };
+    auto yaddr = [](int l, int e) { return XG::off((l / N) * N + e, l % N); };
+    auto xaddr = [](int l, int e) { return YG::off(e * G + l / N, l % N); };
+    for (long long t = 0; t < total; ++t) {
+        const TwoPassItem it = twopass_decode(t, nvol, TG::NA, TG::NB, lag);
+        const int slot = (int)(it.vol % R);
+        const long long round = it.vol / R;
+        cx<T> *sv = ring.data() + slot * TG::V;
+        if (it.plane ? cnt_row[slot] < TG::NB * round : cnt_plane[slot] < TG::NA * (round + 1))
+            g_twopass_violations++;
+        (it.plane ? cnt_plane : cnt_row)[slot]++;
+        for (auto &e : smv) e = {T(12345.0), T(-6789.0)};
+        if (it.plane) {
+            const cx<T> *rows = in + it.vol * TG::V + (long long)it.j * G * PLANE;
+            for (int r = 0; r < G * N; ++r)
+                for (int z = 0; z < N; ++z) sm[XG::off(r, z)] = rows[(long long)r * N + z];
+            for (int q = 0; q < LINES * 9; ++q) pfa36_stage1<S, T>(sm, LINES, q, zaddr);
+            for (int q = 0; q < LINES * 4; ++q)
+                pfa36_stage2<S, T>(sm, LINES, q, zaddr, [&](int l, int k, cx<T> v) { sm[zaddr(l, k)] = v; });
+            for (int q = 0; q < LINES * 9; ++q) pfa36_stage1<S, T>(sm, LINES, q, yaddr);
+            cx<T> *dst = sv + (long long)it.j * G * PLANE;
+            for (int q = 0; q < LINES * 4; ++q)
+                pfa36_stage2<S, T>(sm, LINES, q, yaddr, [&](int l, int k, cx<T> v) {
+                    store_l2(dst + (long long)(l / N) * PLANE + k * N + l % N, v);
+                });
+        } else {
+            for (int q = 0; q < G * N; ++q) {
+                const int x = q / G, yl = q % G;
+                for (int z = 0; z < N; ++z)
+                    sm[YG::off(q, z)] = sv[((long long)x * N + it.j * G + yl) * N + z];
+            }
+            for (int q = 0; q < LINES * 9; ++q) pfa36_stage1<S, T>(sm, LINES, q, xaddr);
+            cx<T> *gvol = out + it.vol * TG::V + (long long)it.j * G * N;
+            for (int q = 0; q < LINES * 4; ++q)
+                pfa36_stage2<S, T>(sm, LINES, q, xaddr, [&](int l, int k, cx<T> v) {
+                    if (S > 0) v = cscale(v, scale);
+                    gvol[k * PLANE + l] = v;
+                });
+        }
+    }
+}
+
 // The split-line TWOPASS variant (SPLIT = true): every pass whose length has a
 // lane split runs split_line_host over whole lines, the host form of the
 // kernel's lane exchange; other axes keep the one-thread-per-line pass.
@@ -256,6 +377,15 @@ typedef void (*emu_fn)(const void *, void *, long long);
      &emulate_twopass_split<N0, N1, N2, T, -1, G>},                                          \
     {N0, N1, N2, sizeof(T) == 8 ? 0 : 1, +1, 400 + G, 1, &emulate_twopass_split<N0, N1, N2, T, +1, G>}
 
+#define EMU_TPR_(N0, N1, N2, G, A, XB, YD)                                                   \
+    {N0, N1, N2, 0, -1, A + G, 1, &emulate_twopass_regs<N0, N1, N2, double, -1, G, XB, YD>},   \
+    {N0, N1, N2, 0, +1, A + G, 1, &emulate_twopass_regs<N0, N1, N2, double, +1, G, XB, YD>}
+#define EMU_TPR(N0, N1, N2, G) EMU_TPR_(N0, N1, N2, G, 500, false, true)
+#define EMU_TPRP(N0, N1, N2, G) EMU_TPR_(N0, N1, N2, G, 520, true, false)
+#define EMU_TPRQ(N0, N1, N2, G) EMU_TPR_(N0, N1, N2, G, 540, true, true)
+#define EMU_TPP(G)                                                                            \
+    {36, 36, 36, 0, -1, 600 + G, 1, &emulate_twopass_pfa<-1, G>},                               \
+    {36, 36, 36, 0, +1, 600 + G, 1, &emulate_twopass_pfa<+1, G>}
 #define EMU_TP(N0, N1, N2, T, G)                                                              \
     {N0, N1, N2, sizeof(T) == 8 ? 0 : 1, -1, 300 + G, 1,                                    \
      &emulate_twopass<N0, N1, N2, T, -1, G>},                                                \
@@ -302,6 +432,9 @@ static const EmuEntry kEmu[] = {
     EMU_TP(64, 64, 64, double, 1), EMU_TP(64, 64, 64, float, 2),
     EMU_TPS(36, 36, 36, double, 2), EMU_TPS(36, 36, 36, double, 1), EMU_TPS(36, 36, 36, float, 4),
     EMU_TPS(64, 64, 64, double, 1), EMU_TPS(64, 64, 64, float, 2),  EMU_TPS(36, 36, 64, double, 2),
+    EMU_TPR(36, 36, 36, 3), EMU_TPR(36, 36, 36, 2), EMU_TPR(36, 36, 36, 4), EMU_TPRP(36, 36, 36, 3), EMU_TPRP(36, 36, 36, 2), EMU_TPRQ(36, 36, 36, 3),
+    EMU_TPRQ(36, 36, 36, 2), EMU_TPRP(45, 45, 45, 3), EMU_TPRP(6, 9, 5, 3), EMU_TPRQ(6, 9, 5, 3), EMU_TPP(2), EMU_TPP(3), EMU_TPP(4),
+    EMU_TPR(6, 9, 5, 3),
 };
 
 // The chain kernel's per-CTA loop (chain_kernels.cu k_chain) for one volume per CTA.

@@ -11,8 +11,8 @@
 // for the plane items of its volume (D steps earlier); a plane item that reuses
 // a slot waits for the row items of the slot's previous volume (step v - R + D,
 // earlier because D < R).  Every wait is on a smaller ticket, which a running
-// CTA holds, so the order cannot deadlock.  With D about one grid's worth of
-// steps, the waits are normally satisfied on arrival, and the ring of R
+// CTA holds, so the order cannot deadlock.  With D about two grids' worth of
+// tickets (twopass_ring), the waits are normally satisfied on arrival, and the ring of R
 // volumes is small enough to stay in L2, so the intermediate costs no HBM
 // traffic: each volume is read from HBM once and written once.
 #pragma once
@@ -75,11 +75,11 @@ FFT_HD TwoPassItem twopass_decode(long long t, long long nvol, int na, int nb, i
     return it;
 }
 
-// Ring geometry for a grid: D = one grid's worth of steps + 2, R = 2D + 2.
-FFT_HD int twopass_ring_size(int na, int nb, long long grid, int *lag)
+// Ring geometry for `held` tickets in flight: D = their worth of steps + 2, R = 2D + 2.
+FFT_HD int twopass_ring_size(int na, int nb, long long held, int *lag)
 {
     const long long ab = na + nb;
-    long long d = (grid + ab - 1) / ab + 2;
+    long long d = (held + ab - 1) / ab + 2;
     const long long dmax = (TWOPASS_RMAX - 2) / 2;
     if (d > dmax) d = dmax;
     *lag = (int)d;

@@ -17,7 +17,10 @@
 // DEV_ERR_DEP_TIMEOUT, raises the workspace abort flag so that the other CTAs
 // stop too, and the last CTA to leave clears the control block for the next
 // launch, on the error path as well.
+#include <algorithm>
+
 #include "internal.h"
+#include "pfa36.cuh"
 #include "ptx.cuh"
 #include "splitline.cuh"
 #include "twopass.cuh"
@@ -451,9 +454,324 @@ __global__ void __launch_bounds__(NT, MINB)
     }
 }
 
+// TWOPASS with lean item control (complex double, row-major layouts).  Thread
+// 0 takes the next ticket while the current item runs, and waits for the
+// current item's dependency (plane items of the volume for a row item; the
+// slot's previous reader for a plane item) before the barrier that starts it;
+// the abort flag is read only inside waits that do not return at once.  A CTA
+// holds at most two tickets and works them in increasing order, so the
+// smallest unfinished ticket always belongs to a CTA that can run it: the
+// ticket-order argument against deadlock still holds.
+//
+// Plane items move their G planes into shared memory by bulk copies and run
+// the z pass there.  The y pass either stores straight into the scratch slot
+// from registers (YDIRECT, L2-only stores; "regs"/"bulkq" in the name) or runs
+// in shared memory, whose rows then go to the slot one warp per row ("bulkp").
+// Row items either load their x-lines straight from the slot into registers
+// (L2-only loads, a warp reading contiguous ranges; no shared memory at all,
+// "regs") or gather their rows by bulk copies first (XBULK, "bulkp"/"bulkq").
+template <int N0, int N1, int N2, int S, int G, int NT, int MINB, bool XBULK = false,
+          bool YDIRECT = true>
+__global__ void __launch_bounds__(NT, MINB)
+    k_twopass_regs(const cx<double> *__restrict__ in, cx<double> *__restrict__ out, long long nvol,
+                   double scale, int *err, unsigned char *work, int R, int D)
+{
+    pdl_begin();
+    using T = double;
+    using TG = TwoPassGeom<N0, N1, N2, T, G>;
+    using XG = typename TG::XG;
+    using YG = typename TG::YG;
+    static_assert(XG::POL != 2 && YG::POL != 2 && NT % 32 == 0, "row-major layouts, whole warps");
+    constexpr uint32_t ROW_BYTES = (uint32_t)(N2 * sizeof(cx<T>));
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);
+    __shared__ long long s_t;
+    __shared__ int s_stop;
+    __shared__ __align__(8) uint64_t s_bar;
+    TwoPassCtl *ctl = reinterpret_cast<TwoPassCtl *>(work);
+    cx<T> *ring = reinterpret_cast<cx<T> *>(work + TWOPASS_CTL_BYTES);
+    const int tid = threadIdx.x;
+    const long long total = (long long)(TG::NA + TG::NB) * nvol;
+    uint32_t phase = 0;
+    bool copies_pending = false;
+    long long next = 0;  // thread 0: the ticket taken ahead
+    if (tid == 0) {
+        mbar_init(&s_bar, 1);
+        fence_mbar_init();
+        next = (long long)atomicAdd(&ctl->ticket, 1ull);
+    }
+    // bounded wait for all bulk copies of the current phase; false on timeout
+    auto wait_copies = [&]() {
+        copies_pending = true;
+        const bool ok = mbar_wait_bounded(&s_bar, phase);
+        phase ^= 1u;
+        if (ok) copies_pending = false;
+        return ok;
+    };
+
+    for (;;) {
+        if (tid == 0) {
+            const long long t = next;
+            int stop = t >= total ? 1 : 0;
+            if (!stop) {
+                next = (long long)atomicAdd(&ctl->ticket, 1ull);
+                const TwoPassItem it = twopass_decode(t, nvol, TG::NA, TG::NB, D);
+                const int slot = (int)(it.vol % R);
+                const unsigned round = (unsigned)(it.vol / R);
+                const unsigned *c = it.plane ? &ctl->cnt[TWOPASS_RMAX + slot] : &ctl->cnt[slot];
+                const unsigned target = it.plane ? (unsigned)TG::NB * round : (unsigned)TG::NA * (round + 1u);
+                if (target > 0 && !wait_counter_geq(c, target, &ctl->abort)) stop = 2;
+            }
+            s_t = t;
+            s_stop = stop;
+        }
+        __syncthreads();
+        if (s_stop) break;
+        const TwoPassItem it = twopass_decode(s_t, nvol, TG::NA, TG::NB, D);
+        const int slot = (int)(it.vol % R);
+        cx<T> *sv = ring + (long long)slot * TG::V;
+
+        if (it.plane) {
+            // 1. G contiguous planes of the input, one bulk copy per row
+            if (tid == 0) mbar_arrive_expect_tx(&s_bar, (uint32_t)XG::ROWS * ROW_BYTES);
+            const cx<T> *rows = in + it.vol * TG::V + (long long)it.j * G * N1 * N2;
+            for (int r = tid; r < XG::ROWS; r += NT)
+                bulk_g2s(sm + XG::off(r, 0), rows + (long long)r * N2, ROW_BYTES, &s_bar);
+            if (!wait_copies()) s_stop = 2;
+            __syncthreads();
+            if (s_stop) break;
+            // 2. z pass in shared memory
+            for (int r = tid; r < XG::ROWS; r += NT) pass_z<XG, S, ALG_DEFAULT>(sm, r);
+            __syncthreads();
+            // 3. y pass into the scratch slot (its previous reader is done: checked above)
+            if constexpr (YDIRECT) {
+                for (int l = tid; l < G * N2; l += NT) pass_y_store_l2<XG, S>(sm, l, sv, it.j * G);
+            } else {
+                for (int l = tid; l < G * N2; l += NT) pass_y<XG, S, ALG_DEFAULT>(sm, l);
+                __syncthreads();
+                cx<T> *dst = sv + (long long)it.j * G * N1 * N2;
+                for (int r = tid / 32; r < XG::ROWS; r += NT / 32)
+                    for (int z = tid % 32; z < N2; z += 32) store_l2(dst + (long long)r * N2 + z, sm[XG::off(r, z)]);
+            }
+            fence_proxy_async_smem();  // these reads before the next item's bulk copies
+            __threadfence();
+            __syncthreads();
+            if (tid == 0) red_release_gpu_add(&ctl->cnt[slot], 1u);
+        } else if constexpr (XBULK) {
+            // 1. the G y-rows of every plane of the slot (its plane items are done)
+            if (tid == 0) mbar_arrive_expect_tx(&s_bar, (uint32_t)(N0 * G) * ROW_BYTES);
+            for (int q = tid; q < N0 * G; q += NT) {
+                const int x = q / G, yl = q % G;
+                fence_proxy_async_global();  // the acquire above precedes these reads
+                bulk_g2s(sm + YG::off(q, 0), sv + ((long long)x * N1 + it.j * G + yl) * N2, ROW_BYTES,
+                         &s_bar);
+            }
+            if (!wait_copies()) s_stop = 2;
+            __syncthreads();
+            if (s_stop) break;
+            // the slot may be overwritten: its rows are in shared memory
+            if (tid == 0) red_release_gpu_add(&ctl->cnt[TWOPASS_RMAX + slot], 1u);
+            // 2. x pass, straight to the output
+            for (int l = tid; l < G * N2; l += NT)
+                pass_x_slab<YG, S, N1>(sm, l, out + it.vol * TG::V, it.j * G, scale);
+            fence_proxy_async_smem();
+            __syncthreads();
+        } else {
+            // x pass from the scratch slot (its plane items are done: checked above)
+            for (int l = tid; l < G * N2; l += NT)
+                pass_x_load_l2<N0, N1, N2, S, T>(sv, l, out + it.vol * TG::V, it.j * G, scale);
+            __syncthreads();  // every load of the slot has returned
+            if (tid == 0) red_release_gpu_add(&ctl->cnt[TWOPASS_RMAX + slot], 1u);
+        }
+    }
+    // a bulk copy that timed out may still land: wait once more (bounded)
+    if (copies_pending) mbar_wait_bounded(&s_bar, phase ^ 1u);
+
+    if (tid == 0 && s_stop == 2) {
+        report_error(err, DEV_ERR_DEP_TIMEOUT);
+        atomicExch(&ctl->abort, 1u);
+    }
+    // The last CTA to leave clears the control block for the next launch.
+    if (tid == 0) {
+        __threadfence();
+        const unsigned prev = atomicAdd(&ctl->done, 1u);
+        if (prev == gridDim.x - 1) {
+            __threadfence();
+            ctl->ticket = 0ull;
+            for (int i = 0; i < 2 * TWOPASS_RMAX; ++i) ctl->cnt[i] = 0u;
+            ctl->abort = 0u;
+            __threadfence();
+            ctl->done = 0u;
+        }
+    }
+}
+
+// TWOPASS for 36^3 complex double with every 36-point line split into its
+// 4 x 9 prime-factor stages (pfa36.cuh): a thread task holds 4 or 9 points, so
+// the kernel runs in ~85 registers and three 256-thread CTAs (24 warps) share
+// an SM, where one-thread-per-line kernels keep 12 warps.  Items, tickets
+// (taken one ahead), waits and bulk row copies as in k_twopass_regs; the y
+// pass's second stage stores into the scratch slot (L2 only), and the row
+// item's rows come back by bulk copies, its second stage streaming the output.
+template <int S, int G, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
+    k_twopass_pfa(const cx<double> *__restrict__ in, cx<double> *__restrict__ out, long long nvol,
+                  double scale, int *err, unsigned char *work, int R, int D)
+{
+    pdl_begin();
+    constexpr int N = 36;
+    using T = double;
+    using TG = TwoPassGeom<N, N, N, T, G>;
+    using XG = typename TG::XG;
+    using YG = typename TG::YG;
+    static_assert(XG::POL == 1 && YG::POL == 1 && NT % 32 == 0, "row pitch 37, whole warps");
+    constexpr uint32_t ROW_BYTES = (uint32_t)(N * sizeof(cx<T>));
+    constexpr int LINES = G * N;  // lines per pass of an item
+    constexpr long long PLANE = (long long)N * N;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);
+    __shared__ long long s_t;
+    __shared__ int s_stop;
+    __shared__ __align__(8) uint64_t s_bar;
+    TwoPassCtl *ctl = reinterpret_cast<TwoPassCtl *>(work);
+    cx<T> *ring = reinterpret_cast<cx<T> *>(work + TWOPASS_CTL_BYTES);
+    const int tid = threadIdx.x;
+    const long long total = (long long)(TG::NA + TG::NB) * nvol;
+    uint32_t phase = 0;
+    bool copies_pending = false;
+    long long next = 0;  // thread 0: the ticket taken ahead
+    if (tid == 0) {
+        mbar_init(&s_bar, 1);
+        fence_mbar_init();
+        next = (long long)atomicAdd(&ctl->ticket, 1ull);
+    }
+    // element e of line l in each pass's layout
+    auto zaddr = [](int l, int e) { return XG::off(l, e); };              // l = row (g, y)
+    auto yaddr = [](int l, int e) { return XG::off((l / N) * N + e, l % N); };  // l = (g, z)
+    auto xaddr = [](int l, int e) { return YG::off(e * G + l / N, l % N); };    // l = (yl, z)
+
+    for (;;) {
+        if (tid == 0) {
+            const long long t = next;
+            int stop = (t >= total || ld_acquire_gpu(&ctl->abort) != 0) ? 1 : 0;
+            if (!stop) {
+                next = (long long)atomicAdd(&ctl->ticket, 1ull);
+                const TwoPassItem it = twopass_decode(t, nvol, TG::NA, TG::NB, D);
+                const int slot = (int)(it.vol % R);
+                const unsigned round = (unsigned)(it.vol / R);
+                const bool ok =
+                    it.plane
+                        ? wait_counter_geq(&ctl->cnt[TWOPASS_RMAX + slot], (unsigned)TG::NB * round,
+                                           &ctl->abort)
+                        : wait_counter_geq(&ctl->cnt[slot], (unsigned)TG::NA * (round + 1u), &ctl->abort);
+                if (!ok) stop = 2;
+            }
+            s_t = t;
+            s_stop = stop;
+        }
+        __syncthreads();
+        if (s_stop) break;
+        const TwoPassItem it = twopass_decode(s_t, nvol, TG::NA, TG::NB, D);
+        const int slot = (int)(it.vol % R);
+        cx<T> *sv = ring + (long long)slot * TG::V;
+
+        // 1. the item's rows, one bulk copy each: G planes of the input, or
+        //    G y-rows of every plane of the scratch slot
+        if (tid == 0) mbar_arrive_expect_tx(&s_bar, (uint32_t)(G * N) * ROW_BYTES);
+        if (it.plane) {
+            const cx<T> *rows = in + it.vol * TG::V + (long long)it.j * G * PLANE;
+            for (int r = tid; r < G * N; r += NT)
+                bulk_g2s(sm + XG::off(r, 0), rows + (long long)r * N, ROW_BYTES, &s_bar);
+        } else {
+            for (int q = tid; q < G * N; q += NT) {
+                const int x = q / G, yl = q % G;
+                fence_proxy_async_global();  // the acquire above precedes these reads
+                bulk_g2s(sm + YG::off(q, 0), sv + ((long long)x * N + it.j * G + yl) * N, ROW_BYTES,
+                         &s_bar);
+            }
+        }
+        copies_pending = true;
+        const bool ok = mbar_wait_bounded(&s_bar, phase);
+        phase ^= 1u;
+        if (!ok) s_stop = 2;
+        else copies_pending = false;
+        __syncthreads();
+        if (s_stop) break;
+
+        if (it.plane) {
+            // 2. z pass, both stages in place
+            for (int t = tid; t < LINES * 9; t += NT) pfa36_stage1<S, T>(sm, LINES, t, zaddr);
+            __syncthreads();
+            for (int t = tid; t < LINES * 4; t += NT)
+                pfa36_stage2<S, T>(sm, LINES, t, zaddr, [&](int l, int k, cx<T> v) { sm[zaddr(l, k)] = v; });
+            __syncthreads();
+            // 3. y pass; its second stage stores into the scratch slot
+            for (int t = tid; t < LINES * 9; t += NT) pfa36_stage1<S, T>(sm, LINES, t, yaddr);
+            __syncthreads();
+            cx<T> *dst = sv + (long long)it.j * G * PLANE;
+            for (int t = tid; t < LINES * 4; t += NT)
+                pfa36_stage2<S, T>(sm, LINES, t, yaddr, [&](int l, int k, cx<T> v) {
+                    store_l2(dst + (long long)(l / N) * PLANE + k * N + l % N, v);
+                });
+            fence_proxy_async_smem();  // these reads before the next item's bulk copies
+            __threadfence();
+            __syncthreads();
+            if (tid == 0) red_release_gpu_add(&ctl->cnt[slot], 1u);
+        } else {
+            // the slot's rows are in shared memory: it may be overwritten
+            if (tid == 0) red_release_gpu_add(&ctl->cnt[TWOPASS_RMAX + slot], 1u);
+            // 2. x pass; its second stage streams the output
+            for (int t = tid; t < LINES * 9; t += NT) pfa36_stage1<S, T>(sm, LINES, t, xaddr);
+            __syncthreads();
+            cx<T> *gvol = out + it.vol * TG::V + (long long)it.j * G * N;
+            for (int t = tid; t < LINES * 4; t += NT)
+                pfa36_stage2<S, T>(sm, LINES, t, xaddr, [&](int l, int k, cx<T> v) {
+                    if constexpr (S > 0) v = cscale(v, scale);
+                    store_out(gvol + k * PLANE + l, v);
+                });
+            fence_proxy_async_smem();
+            __syncthreads();
+        }
+    }
+    // a bulk copy that timed out may still land: wait once more (bounded)
+    if (copies_pending) mbar_wait_bounded(&s_bar, phase ^ 1u);
+
+    if (tid == 0 && s_stop == 2) {
+        report_error(err, DEV_ERR_DEP_TIMEOUT);
+        atomicExch(&ctl->abort, 1u);
+    }
+    // The last CTA to leave clears the control block for the next launch.
+    if (tid == 0) {
+        __threadfence();
+        const unsigned prev = atomicAdd(&ctl->done, 1u);
+        if (prev == gridDim.x - 1) {
+            __threadfence();
+            ctl->ticket = 0ull;
+            for (int i = 0; i < 2 * TWOPASS_RMAX; ++i) ctl->cnt[i] = 0u;
+            ctl->abort = 0u;
+            __threadfence();
+            ctl->done = 0u;
+        }
+    }
+}
+
 int twopass_ring(const KernelEntry &e, long long grid, int *lag)
 {
-    return twopass_ring_size(e.n0 / e.vpc, e.n1 / e.vpc, grid, lag);
+    // The lag covers up to twice the tickets the grid holds at once: kernels
+    // that take their next ticket ahead (k_twopass_regs, k_twopass_pfa) hold
+    // two per CTA, and for the others too a lag of two grids' worth measured
+    // faster on B200 (fewer row items arriving before their planes are done).
+    // It is shortened, down to one grid's worth, while the ring would exceed
+    // 64 MB, so that the ring stays in half of L2.
+    const int na = e.n0 / e.vpc, nb = e.n1 / e.vpc;
+    const long long vbytes = (long long)e.n0 * e.n1 * e.n2 * element_bytes(e.precision);
+    long long held = 2 * grid;
+    int r = twopass_ring_size(na, nb, held, lag);
+    while (held > grid && (long long)r * vbytes > (64LL << 20)) {
+        held = std::max(grid, held - (long long)(na + nb));
+        r = twopass_ring_size(na, nb, held, lag);
+    }
+    return r;
 }
 
 size_t entry_workspace_bytes(const KernelEntry &e, int grid_limit)
@@ -509,6 +827,70 @@ static void add_twopass_pipe(std::vector<KernelEntry> &out, const char *name)
     out.push_back(e);
 }
 
+template <int N0, int N1, int N2, int S, int G, int NT, int MINB, bool XBULK = false, bool YDIRECT = true>
+static void add_twopass_regs(std::vector<KernelEntry> &out, const char *name)
+{
+    using TG = TwoPassGeom<N0, N1, N2, double, G>;
+    using XG = typename TG::XG;
+    KernelEntry e;
+    e.n0 = N0;
+    e.n1 = N1;
+    e.n2 = N2;
+    e.precision = FFT3D_B200_C128;
+    e.sign = S;
+    e.family = FAM_TWOPASS;  // same launch arguments and workspace as k_twopass
+    e.alg = 8 + (XBULK ? 32 : 0) + (YDIRECT ? 0 : 64);
+    e.vpc = G;
+    e.threads = NT;
+    // plane items only, unless row items gather their rows into shared memory too
+    e.smem = XBULK ? TG::SMEM : ((XG::PV * XG::EB) + 127) / 128 * 128;
+    e.func = (const void *)&k_twopass_regs<N0, N1, N2, S, G, NT, MINB, XBULK, YDIRECT>;
+    e.name = name;
+    out.push_back(e);
+}
+
+// Passes straight between registers and L2, complex double: "regs" in the name.
+#define FFT3D_TWOPASS_REGS(N0, N1, N2, G, NT, MINB)                                              \
+    add_twopass_regs<N0, N1, N2, -1, G, NT, MINB>(out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G \
+                                                       " regs nt" #NT " minb" #MINB);              \
+    add_twopass_regs<N0, N1, N2, +1, G, NT, MINB>(out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G \
+                                                       " regs nt" #NT " minb" #MINB)
+
+// Lean control with bulk row gathers: "bulkp" (y pass in shared memory, rows
+// stored by warps) and "bulkq" (y pass stored from registers).
+#define FFT3D_TWOPASS_BULKP(N0, N1, N2, G, NT, MINB)                                             \
+    add_twopass_regs<N0, N1, N2, -1, G, NT, MINB, true, false>(                                  \
+        out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G " bulkp nt" #NT " minb" #MINB);       \
+    add_twopass_regs<N0, N1, N2, +1, G, NT, MINB, true, false>(                                  \
+        out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G " bulkp nt" #NT " minb" #MINB)
+#define FFT3D_TWOPASS_BULKQ(N0, N1, N2, G, NT, MINB)                                             \
+    add_twopass_regs<N0, N1, N2, -1, G, NT, MINB, true, true>(                                   \
+        out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G " bulkq nt" #NT " minb" #MINB);       \
+    add_twopass_regs<N0, N1, N2, +1, G, NT, MINB, true, true>(                                   \
+        out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G " bulkq nt" #NT " minb" #MINB)
+
+template <int S, int G, int NT, int MINB>
+static void add_twopass_pfa(std::vector<KernelEntry> &out, const char *name)
+{
+    KernelEntry e;
+    e.n0 = e.n1 = e.n2 = 36;
+    e.precision = FFT3D_B200_C128;
+    e.sign = S;
+    e.family = FAM_TWOPASS;  // same launch arguments and workspace as k_twopass
+    e.alg = 16;
+    e.vpc = G;
+    e.threads = NT;
+    e.smem = TwoPassGeom<36, 36, 36, double, G>::SMEM;
+    e.func = (const void *)&k_twopass_pfa<S, G, NT, MINB>;
+    e.name = name;
+    out.push_back(e);
+}
+
+// 36^3 complex double, lines split into their 4 x 9 stages: "pfa" in the name.
+#define FFT3D_TWOPASS_PFA36(G, NT, MINB)                                                           \
+    add_twopass_pfa<-1, G, NT, MINB>(out, "twopass 36x36x36 double g" #G " pfa nt" #NT " minb" #MINB); \
+    add_twopass_pfa<+1, G, NT, MINB>(out, "twopass 36x36x36 double g" #G " pfa nt" #NT " minb" #MINB)
+
 // Rows moved by bulk copies (complex double, row-major layouts): "bulk" in the name.
 #define FFT3D_TWOPASS_BULK(N0, N1, N2, G, NT, MINB)                                              \
     add_twopass<N0, N1, N2, double, -1, G, NT, MINB, false, true>(                               \
@@ -532,6 +914,23 @@ static void add_twopass_pipe(std::vector<KernelEntry> &out, const char *name)
 
 void register_twopass_kernels(std::vector<KernelEntry> &out)
 {
+    // lean control: next ticket taken ahead, dependency waited at the top
+    FFT3D_TWOPASS_BULKP(36, 36, 36, 3, 128, 3);
+    FFT3D_TWOPASS_BULKP(36, 36, 36, 2, 96, 4);
+    FFT3D_TWOPASS_BULKQ(36, 36, 36, 3, 128, 3);
+    FFT3D_TWOPASS_BULKQ(36, 36, 36, 2, 96, 4);
+    FFT3D_TWOPASS_BULKP(45, 45, 45, 3, 160, 2);
+    // 36-point lines as 4 x 9 stages: ~85 registers, 24 warps per SM
+    FFT3D_TWOPASS_PFA36(3, 256, 3);
+    FFT3D_TWOPASS_PFA36(2, 256, 4);
+    FFT3D_TWOPASS_PFA36(4, 256, 2);
+    FFT3D_TWOPASS_PFA36(3, 384, 2);
+    FFT3D_TWOPASS_PFA36(2, 192, 5);
+    // z pass in shared memory, y and x passes between registers and L2
+    FFT3D_TWOPASS_REGS(36, 36, 36, 3, 128, 3);
+    FFT3D_TWOPASS_REGS(36, 36, 36, 2, 96, 4);
+    FFT3D_TWOPASS_REGS(36, 36, 36, 4, 160, 2);
+    FFT3D_TWOPASS_REGS(36, 36, 36, 2, 96, 3);  // 227 registers: no spills, 9 warps
     // rows moved by bulk copies: almost no integer work outside the transform
     FFT3D_TWOPASS_BULK(36, 36, 36, 2, 96, 4);
     FFT3D_TWOPASS_BULK(36, 36, 36, 3, 128, 3);  // 108 lines on 4 warps: 84% of lanes busy

@@ -199,6 +199,75 @@ FFT_HD void pass_x_slab(const cx<typename G::T> *sm, int l, cx<typename G::T> *g
     }
 }
 
+// L2-only accesses, for buffers that other SMs write during the launch (the
+// per-SM L1 is not coherent with them).  Plain accesses on the host.
+template <typename T>
+FFT_HD void store_l2(cx<T> *p, cx<T> v)
+{
+#if defined(__CUDA_ARCH__)
+    if constexpr (sizeof(T) == 8) __stcg(reinterpret_cast<double2 *>(p), make_double2(v.re, v.im));
+    else __stcg(reinterpret_cast<float2 *>(p), make_float2(v.re, v.im));
+#else
+    *p = v;
+#endif
+}
+
+template <typename T>
+FFT_HD cx<T> load_l2(const cx<T> *p)
+{
+#if defined(__CUDA_ARCH__)
+    if constexpr (sizeof(T) == 8) {
+        const double2 t = __ldcg(reinterpret_cast<const double2 *>(p));
+        return {t.x, t.y};
+    } else {
+        const float2 t = __ldcg(reinterpret_cast<const float2 *>(p));
+        return {t.x, t.y};
+    }
+#else
+    return *p;
+#endif
+}
+
+// Pass along y for line l = g*N2 + z of a block of planes G = (planes, N1, N2)
+// in shared memory, written straight to a volume-shaped buffer whose plane g
+// is plane x0 + g, with L2-only stores.  Consecutive l are consecutive z, so
+// each store instruction of a warp covers contiguous ranges.
+template <class G, int S>
+FFT_HD void pass_y_store_l2(const cx<typename G::T> *sm, int l, cx<typename G::T> *gvol, int x0)
+{
+    using T = typename G::T;
+    const int z = l % G::N2;
+    const int g = l / G::N2;
+    cx<T> v[G::N1];
+#pragma unroll
+    for (int j = 0; j < G::N1; ++j) v[j] = sm[G::off(g * G::N1 + j, z)];
+    dft<G::N1, S, T>(v);
+    cx<T> *o = gvol + (long long)(x0 + g) * G::N1 * G::N2 + z;
+#pragma unroll
+    for (int j = 0; j < G::N1; ++j) store_l2(o + j * G::N2, v[j]);
+}
+
+// Pass along x for line l of y-rows [y0, ...) of an N0 x N1 x N2 volume-shaped
+// buffer, read straight from it with L2-only loads (line l is the point
+// (y0*N2 + l) of every plane: consecutive l are consecutive addresses) and
+// streamed to gvol at the same offsets.
+template <int N0, int N1, int N2, int S, typename T>
+FFT_HD void pass_x_load_l2(const cx<T> *src, int l, cx<T> *gvol, int y0, T scale)
+{
+    constexpr long long PLANE = (long long)N1 * N2;
+    const long long e = (long long)y0 * N2 + l;
+    cx<T> v[N0];
+#pragma unroll
+    for (int j = 0; j < N0; ++j) v[j] = load_l2(src + j * PLANE + e);
+    dft<N0, S, T>(v);
+#pragma unroll
+    for (int j = 0; j < N0; ++j) {
+        cx<T> r = v[j];
+        if constexpr (S > 0) r = cscale(r, scale);
+        store_out(gvol + j * PLANE + e, r);
+    }
+}
+
 // Copy element g (in [0, nv*V)) of the CTA's input slice into its layout slot.
 template <class G>
 FFT_HD void stage_in(cx<typename G::T> *sm, const cx<typename G::T> *gin, int g)

@@ -127,6 +127,52 @@ def test_twopass_items(hostcheck, shape, prec, g, nvol, sign):
     assert err < (C128_TOL if prec == 0 else C64_TOL), err
 
 
+REGS = [((36, 36, 36), 500, 3, 7), ((36, 36, 36), 500, 2, 11), ((36, 36, 36), 500, 4, 3),
+        ((6, 9, 5), 500, 3, 41), ((36, 36, 36), 520, 3, 7), ((36, 36, 36), 520, 2, 5),
+        ((36, 36, 36), 540, 3, 6), ((36, 36, 36), 540, 2, 3), ((45, 45, 45), 520, 3, 3),
+        ((6, 9, 5), 520, 3, 41), ((6, 9, 5), 540, 3, 41)]
+
+
+@pytest.mark.parametrize("shape,base,g,nvol", REGS,
+                         ids=[f"{t[0]}-a{t[1]}-g{t[2]}-b{t[3]}" for t in REGS])
+@pytest.mark.parametrize("sign", [-1, +1])
+def test_twopass_lean_control_variants(hostcheck, shape, base, g, nvol, sign):
+    """The lean-control TWOPASS variants: y pass stored straight into the
+    scratch slot and x pass loaded straight from it (alg = 500 + G), y pass in
+    shared memory with row copies and bulk-gathered x pass (520 + G), y pass
+    from registers with bulk-gathered x pass (540 + G); the line maps of
+    pass_y_store_l2 / pass_x_load_l2, in ticket order with the dependency check."""
+    import ctypes
+    hostcheck.hostcheck_twopass_violations.restype = ctypes.c_longlong
+    hostcheck.hostcheck_twopass_violations()
+    rng = np.random.default_rng(7000 + g + nvol + sum(shape))
+    x = field(rng, (nvol,) + shape, dist="normal")
+    got = run(hostcheck, x, shape, 0, sign, base + g, 1)
+    assert hostcheck.hostcheck_twopass_violations() == 0
+    want = oracle.fft3d(x) if sign < 0 else oracle.ifft3d(x)
+    assert oracle.rel_error_per_volume(got, want).max() < C128_TOL
+
+
+PFA = [(3, 7), (2, 11), (4, 3), (3, 1)]
+
+
+@pytest.mark.parametrize("g,nvol", PFA, ids=[f"g{t[0]}-b{t[1]}" for t in PFA])
+@pytest.mark.parametrize("sign", [-1, +1])
+def test_twopass_pfa36_stages(hostcheck, g, nvol, sign):
+    """36^3 TWOPASS with every line split into its 4 x 9 Good-Thomas stages
+    (alg = 600 + G): the index maps of pfa36.cuh, the in-place stage order and
+    the three pass layouts, in ticket order with the dependency check."""
+    import ctypes
+    hostcheck.hostcheck_twopass_violations.restype = ctypes.c_longlong
+    hostcheck.hostcheck_twopass_violations()
+    rng = np.random.default_rng(8000 + g + nvol)
+    x = field(rng, (nvol, 36, 36, 36), dist="normal")
+    got = run(hostcheck, x, (36, 36, 36), 0, sign, 600 + g, 1)
+    assert hostcheck.hostcheck_twopass_violations() == 0
+    want = oracle.fft3d(x) if sign < 0 else oracle.ifft3d(x)
+    assert oracle.rel_error_per_volume(got, want).max() < C128_TOL
+
+
 SPLIT = [((36, 36, 36), 0, 2, 11), ((36, 36, 36), 0, 1, 3), ((36, 36, 36), 1, 4, 5),
          ((64, 64, 64), 0, 1, 3), ((64, 64, 64), 1, 2, 2), ((36, 36, 64), 0, 2, 4)]
 

@@ -471,7 +471,7 @@ __global__ void __launch_bounds__(NT, MINB)
 // (L2-only loads, a warp reading contiguous ranges; no shared memory at all,
 // "regs") or gather their rows by bulk copies first (XBULK, "bulkp"/"bulkq").
 template <int N0, int N1, int N2, int S, int G, int NT, int MINB, bool XBULK = false,
-          bool YDIRECT = true>
+          bool YDIRECT = true, bool HINT = false>
 __global__ void __launch_bounds__(NT, MINB)
     k_twopass_regs(const cx<double> *__restrict__ in, cx<double> *__restrict__ out, long long nvol,
                    double scale, int *err, unsigned char *work, int R, int D)
@@ -495,6 +495,11 @@ __global__ void __launch_bounds__(NT, MINB)
     uint32_t phase = 0;
     bool copies_pending = false;
     long long next = 0;  // thread 0: the ticket taken ahead
+    uint64_t pol_first = 0, pol_last = 0;
+    if constexpr (HINT) {
+        pol_first = l2_policy_evict_first();
+        pol_last = l2_policy_evict_last();
+    }
     if (tid == 0) {
         mbar_init(&s_bar, 1);
         fence_mbar_init();
@@ -535,8 +540,12 @@ __global__ void __launch_bounds__(NT, MINB)
             // 1. G contiguous planes of the input, one bulk copy per row
             if (tid == 0) mbar_arrive_expect_tx(&s_bar, (uint32_t)XG::ROWS * ROW_BYTES);
             const cx<T> *rows = in + it.vol * TG::V + (long long)it.j * G * N1 * N2;
-            for (int r = tid; r < XG::ROWS; r += NT)
-                bulk_g2s(sm + XG::off(r, 0), rows + (long long)r * N2, ROW_BYTES, &s_bar);
+            for (int r = tid; r < XG::ROWS; r += NT) {
+                if constexpr (HINT)  // read once: do not displace the ring
+                    bulk_g2s_hint(sm + XG::off(r, 0), rows + (long long)r * N2, ROW_BYTES, &s_bar, pol_first);
+                else
+                    bulk_g2s(sm + XG::off(r, 0), rows + (long long)r * N2, ROW_BYTES, &s_bar);
+            }
             if (!wait_copies()) s_stop = 2;
             __syncthreads();
             if (s_stop) break;
@@ -544,7 +553,19 @@ __global__ void __launch_bounds__(NT, MINB)
             for (int r = tid; r < XG::ROWS; r += NT) pass_z<XG, S, ALG_DEFAULT>(sm, r);
             __syncthreads();
             // 3. y pass into the scratch slot (its previous reader is done: checked above)
-            if constexpr (YDIRECT) {
+            if constexpr (YDIRECT && HINT) {
+                // ring lines stay in L2 (evict_last): a slot is rewritten in L2, not written back
+                for (int l = tid; l < G * N2; l += NT) {
+                    const int z = l % N2, g = l / N2;
+                    cx<T> v[N1];
+#pragma unroll
+                    for (int j = 0; j < N1; ++j) v[j] = sm[XG::off(g * N1 + j, z)];
+                    dft<N1, S, T>(v);
+                    double2 *o = reinterpret_cast<double2 *>(sv + (long long)(it.j * G + g) * N1 * N2 + z);
+#pragma unroll
+                    for (int j = 0; j < N1; ++j) st_cg_hint(o + j * N2, make_double2(v[j].re, v[j].im), pol_last);
+                }
+            } else if constexpr (YDIRECT) {
                 for (int l = tid; l < G * N2; l += NT) pass_y_store_l2<XG, S>(sm, l, sv, it.j * G);
             } else {
                 for (int l = tid; l < G * N2; l += NT) pass_y<XG, S, ALG_DEFAULT>(sm, l);
@@ -827,7 +848,8 @@ static void add_twopass_pipe(std::vector<KernelEntry> &out, const char *name)
     out.push_back(e);
 }
 
-template <int N0, int N1, int N2, int S, int G, int NT, int MINB, bool XBULK = false, bool YDIRECT = true>
+template <int N0, int N1, int N2, int S, int G, int NT, int MINB, bool XBULK = false, bool YDIRECT = true,
+          bool HINT = false>
 static void add_twopass_regs(std::vector<KernelEntry> &out, const char *name)
 {
     using TG = TwoPassGeom<N0, N1, N2, double, G>;
@@ -839,12 +861,12 @@ static void add_twopass_regs(std::vector<KernelEntry> &out, const char *name)
     e.precision = FFT3D_B200_C128;
     e.sign = S;
     e.family = FAM_TWOPASS;  // same launch arguments and workspace as k_twopass
-    e.alg = 8 + (XBULK ? 32 : 0) + (YDIRECT ? 0 : 64);
+    e.alg = 8 + (XBULK ? 32 : 0) + (YDIRECT ? 0 : 64) + (HINT ? 128 : 0);
     e.vpc = G;
     e.threads = NT;
     // plane items only, unless row items gather their rows into shared memory too
     e.smem = XBULK ? TG::SMEM : ((XG::PV * XG::EB) + 127) / 128 * 128;
-    e.func = (const void *)&k_twopass_regs<N0, N1, N2, S, G, NT, MINB, XBULK, YDIRECT>;
+    e.func = (const void *)&k_twopass_regs<N0, N1, N2, S, G, NT, MINB, XBULK, YDIRECT, HINT>;
     e.name = name;
     out.push_back(e);
 }
@@ -863,6 +885,12 @@ static void add_twopass_regs(std::vector<KernelEntry> &out, const char *name)
         out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G " bulkp nt" #NT " minb" #MINB);       \
     add_twopass_regs<N0, N1, N2, +1, G, NT, MINB, true, false>(                                  \
         out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G " bulkp nt" #NT " minb" #MINB)
+// bulkq with L2 policies: input planes evict_first, ring stores evict_last ("bulkqh").
+#define FFT3D_TWOPASS_BULKQH(N0, N1, N2, G, NT, MINB)                                            \
+    add_twopass_regs<N0, N1, N2, -1, G, NT, MINB, true, true, true>(                             \
+        out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G " bulkqh nt" #NT " minb" #MINB);      \
+    add_twopass_regs<N0, N1, N2, +1, G, NT, MINB, true, true, true>(                             \
+        out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G " bulkqh nt" #NT " minb" #MINB)
 #define FFT3D_TWOPASS_BULKQ(N0, N1, N2, G, NT, MINB)                                             \
     add_twopass_regs<N0, N1, N2, -1, G, NT, MINB, true, true>(                                   \
         out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G " bulkq nt" #NT " minb" #MINB);       \
@@ -915,6 +943,8 @@ static void add_twopass_pfa(std::vector<KernelEntry> &out, const char *name)
 void register_twopass_kernels(std::vector<KernelEntry> &out)
 {
     // lean control: next ticket taken ahead, dependency waited at the top
+    FFT3D_TWOPASS_BULKQH(36, 36, 36, 3, 128, 3);
+    FFT3D_TWOPASS_BULKQH(36, 36, 36, 2, 96, 4);
     FFT3D_TWOPASS_BULKP(36, 36, 36, 3, 128, 3);
     FFT3D_TWOPASS_BULKP(36, 36, 36, 2, 96, 4);
     FFT3D_TWOPASS_BULKQ(36, 36, 36, 3, 128, 3);

@@ -57,7 +57,25 @@ WORKLOADS = {
                      label="4096 x 8^3 complex64 forward"),
     "fwd16_c64": dict(shape=(16, 16, 16), batch=1024, prec=1, chain=(-1,), dist="uniform",
                       label="1024 x 16^3 complex64 forward"),
+    # the further extents (not in the default run: --extras f4)
+    "fwd13": dict(shape=(13, 13, 13), batch=8192, prec=0, chain=(-1,), dist="uniform",
+                  label="8192 x 13^3 complex128 forward"),
+    "fwd23": dict(shape=(23, 23, 23), batch=1024, prec=0, chain=(-1,), dist="uniform",
+                  label="1024 x 23^3 complex128 forward"),
+    "fwd45": dict(shape=(45, 45, 45), batch=128, prec=0, chain=(-1,), dist="normal",
+                  label="128 x 45^3 complex128 forward"),
+    "fwd64": dict(shape=(64, 64, 64), batch=64, prec=0, chain=(-1,), dist="normal",
+                  label="64 x 64^3 complex128 forward"),
+    "fwd13_c64": dict(shape=(13, 13, 13), batch=8192, prec=1, chain=(-1,), dist="uniform",
+                      label="8192 x 13^3 complex64 forward"),
+    "fwd23_c64": dict(shape=(23, 23, 23), batch=1024, prec=1, chain=(-1,), dist="uniform",
+                      label="1024 x 23^3 complex64 forward"),
+    "fwd45_c64": dict(shape=(45, 45, 45), batch=128, prec=1, chain=(-1,), dist="normal",
+                      label="128 x 45^3 complex64 forward"),
+    "fwd64_c64": dict(shape=(64, 64, 64), batch=64, prec=1, chain=(-1,), dist="normal",
+                      label="64 x 64^3 complex64 forward"),
 }
+F4 = ["fwd13", "fwd23", "fwd45", "fwd64", "fwd13_c64", "fwd23_c64", "fwd45_c64", "fwd64_c64"]
 EXTRA = ["fwd8", "fwd17", "fwd36", "fwd16x16x32", "fwd8_c64", "fwd16_c64"]
 
 
@@ -593,7 +611,8 @@ def main():
     ap.add_argument("--workload", default="roundtrip17", choices=sorted(WORKLOADS))
     ap.add_argument("--no-extra", action="store_true", help="skip the per-L workloads")
     ap.add_argument("--extras", default="all",
-                    help="comma list of the per-L workloads to run (default all, incl. mixed_c64)")
+                    help="comma list of the per-L workloads to run (default all, incl. mixed_c64; "
+                         "f4: the 13, 23, 45, 64 extents in both precisions)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0,
                     help="CPU baseline sample length; 0 skips it")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-pointer measurement")
@@ -674,7 +693,7 @@ def main():
 
     workloads = {}
     extras = (EXTRA + ["mixed_c64", "chain", "serve"] if a.extras == "all"
-              else [e for e in a.extras.split(",") if e])
+              else F4 if a.extras == "f4" else [e for e in a.extras.split(",") if e])
     if not a.no_extra:
         for name in extras:
             if name not in WORKLOADS:

@@ -944,6 +944,8 @@ void register_twopass_kernels(std::vector<KernelEntry> &out)
 {
     // lean control: next ticket taken ahead, dependency waited at the top
     FFT3D_TWOPASS_BULKQH(36, 36, 36, 3, 128, 3);
+    FFT3D_TWOPASS_BULKQH(45, 45, 45, 3, 160, 2);
+    FFT3D_TWOPASS_BULKQH(45, 45, 45, 5, 256, 1);
     FFT3D_TWOPASS_BULKQH(36, 36, 36, 2, 96, 4);
     FFT3D_TWOPASS_BULKP(36, 36, 36, 3, 128, 3);
     FFT3D_TWOPASS_BULKP(36, 36, 36, 2, 96, 4);

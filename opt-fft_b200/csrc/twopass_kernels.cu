@@ -8,8 +8,11 @@
 // stores; a row item reads its G y-rows of all planes back with L2-only loads
 // (never through L1, which is not coherent with other SMs' stores), runs the
 // x pass and streams the result to the output.  Completion is published per
-// slot with a release add after a CTA-wide barrier and a fence, and observed
-// with an acquire load, by one thread, before a barrier.  Several CTAs per SM
+// slot by one thread's gpu-scope release add after a CTA-wide barrier -- the
+// release is cumulative (PTX memory model: causality order runs through the
+// barrier), so it publishes every thread's stores and no thread needs a fence
+// of its own -- and observed with an acquire load, by one thread, before a
+// barrier.  Several CTAs per SM
 // (small items) overlap one another's loads, arithmetic and stores, so unlike
 // a thread-block cluster that moves one volume in lock-step, HBM stays busy.
 //
@@ -229,8 +232,7 @@ __global__ void __launch_bounds__(NT, MINB)
                     st_l2(sv + vo, sm[so]);
                 }
             }
-            __threadfence();
-            __syncthreads();
+            __syncthreads();  // then one cumulative release publishes every thread's stores
             if (tid == 0) red_release_gpu_add(&ctl->cnt[slot], 1u);
         } else {
             // 1. all plane items of this volume must be in scratch
@@ -413,8 +415,7 @@ __global__ void __launch_bounds__(NT, MINB)
                 twopass_plane_elem<TG>(it.j, g, &vo, &so);
                 st_l2(sv + vo, sm[so]);
             }
-            __threadfence();
-            __syncthreads();
+            __syncthreads();  // then one cumulative release publishes every thread's stores
             if (tid == 0) red_release_gpu_add(&ctl->cnt[slot], 1u);
         } else {
             // the copies of this row item are complete: its slot may be reused
@@ -575,8 +576,7 @@ __global__ void __launch_bounds__(NT, MINB)
                     for (int z = tid % 32; z < N2; z += 32) store_l2(dst + (long long)r * N2 + z, sm[XG::off(r, z)]);
             }
             fence_proxy_async_smem();  // these reads before the next item's bulk copies
-            __threadfence();
-            __syncthreads();
+            __syncthreads();  // then one cumulative release publishes every thread's stores
             if (tid == 0) red_release_gpu_add(&ctl->cnt[slot], 1u);
         } else if constexpr (XBULK) {
             // 1. the G y-rows of every plane of the slot (its plane items are done)
@@ -735,8 +735,7 @@ __global__ void __launch_bounds__(NT, MINB)
                     store_l2(dst + (long long)(l / N) * PLANE + k * N + l % N, v);
                 });
             fence_proxy_async_smem();  // these reads before the next item's bulk copies
-            __threadfence();
-            __syncthreads();
+            __syncthreads();  // then one cumulative release publishes every thread's stores
             if (tid == 0) red_release_gpu_add(&ctl->cnt[slot], 1u);
         } else {
             // the slot's rows are in shared memory: it may be overwritten

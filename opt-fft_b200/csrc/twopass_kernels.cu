@@ -12,9 +12,9 @@
 // release is cumulative (PTX memory model: causality order runs through the
 // barrier), so it publishes every thread's stores and no thread needs a fence
 // of its own -- and observed with an acquire load, by one thread, before a
-// barrier.  Several CTAs per SM
-// (small items) overlap one another's loads, arithmetic and stores, so unlike
-// a thread-block cluster that moves one volume in lock-step, HBM stays busy.
+// barrier.  Several CTAs per SM (small items) overlap one another's loads,
+// arithmetic and stores, so unlike a thread-block cluster that moves one
+// volume in lock-step, HBM stays busy.
 //
 // Every wait is bounded in time (ptx.cuh wait_counter_geq); a timeout records
 // DEV_ERR_DEP_TIMEOUT, raises the workspace abort flag so that the other CTAs
@@ -456,10 +456,11 @@ __global__ void __launch_bounds__(NT, MINB)
 }
 
 // TWOPASS with lean item control (complex double, row-major layouts).  Thread
-// 0 takes the next ticket while the current item runs, and waits for the
-// current item's dependency (plane items of the volume for a row item; the
-// slot's previous reader for a plane item) before the barrier that starts it;
-// the abort flag is read only inside waits that do not return at once.  A CTA
+// 0 takes the next ticket while the current item runs.  A row item's
+// dependency (the plane items of its volume) is waited for before the barrier
+// that starts it; a plane item's (the slot's previous reader) while its input
+// rows are in flight, before the y pass stores into the slot.  The abort flag
+// is read only inside waits that do not return at once.  A CTA
 // holds at most two tickets and works them in increasing order, so the
 // smallest unfinished ticket always belongs to a CTA that can run it: the
 // ticket-order argument against deadlock still holds.
@@ -522,11 +523,9 @@ __global__ void __launch_bounds__(NT, MINB)
             if (!stop) {
                 next = (long long)atomicAdd(&ctl->ticket, 1ull);
                 const TwoPassItem it = twopass_decode(t, nvol, TG::NA, TG::NB, D);
-                const int slot = (int)(it.vol % R);
-                const unsigned round = (unsigned)(it.vol / R);
-                const unsigned *c = it.plane ? &ctl->cnt[TWOPASS_RMAX + slot] : &ctl->cnt[slot];
-                const unsigned target = it.plane ? (unsigned)TG::NB * round : (unsigned)TG::NA * (round + 1u);
-                if (target > 0 && !wait_counter_geq(c, target, &ctl->abort)) stop = 2;
+                // a row item reads its slot: its plane items must be done first
+                const unsigned target = (unsigned)TG::NA * (unsigned)(it.vol / R + 1);
+                if (!it.plane && !wait_counter_geq(&ctl->cnt[it.vol % R], target, &ctl->abort)) stop = 2;
             }
             s_t = t;
             s_stop = stop;
@@ -547,13 +546,20 @@ __global__ void __launch_bounds__(NT, MINB)
                 else
                     bulk_g2s(sm + XG::off(r, 0), rows + (long long)r * N2, ROW_BYTES, &s_bar);
             }
+            // while the rows are in flight: the slot's previous volume must have
+            // been read out before this item's y pass stores into it
+            if (tid == 0) {
+                const unsigned target = (unsigned)TG::NB * (unsigned)(it.vol / R);
+                if (target > 0 && !wait_counter_geq(&ctl->cnt[TWOPASS_RMAX + slot], target, &ctl->abort))
+                    s_stop = 2;
+            }
             if (!wait_copies()) s_stop = 2;
             __syncthreads();
             if (s_stop) break;
             // 2. z pass in shared memory
             for (int r = tid; r < XG::ROWS; r += NT) pass_z<XG, S, ALG_DEFAULT>(sm, r);
             __syncthreads();
-            // 3. y pass into the scratch slot (its previous reader is done: checked above)
+            // 3. y pass into the scratch slot (its previous reader is done: checked in step 1)
             if constexpr (YDIRECT && HINT) {
                 // ring lines stay in L2 (evict_last): a slot is rewritten in L2, not written back
                 for (int l = tid; l < G * N2; l += NT) {

@@ -11,6 +11,7 @@
 
 #include <vector>
 
+#include "ct64.cuh"
 #include "mgpu.cuh"
 #include "pfa36.cuh"
 #include "splitline.cuh"
@@ -295,6 +296,63 @@ static void emulate_twopass_pfa(const void *vin, void *vout, long long nvol)
     }
 }
 
+// The 64^3 TWOPASS variant with lines split into 8 x 8 stages
+// (k_twopass_ct64): rows at pitch 65, z pass in place (rows end in ct64_slot
+// order), y pass stored into the slot at the natural z, x pass streamed out;
+// every stage-1 task of a pass before any stage-2 task, as the kernel's
+// barrier orders them.  Tickets, ring and dependency checks as emulate_twopass.
+template <int S>
+static void emulate_twopass_ct64(const void *vin, void *vout, long long nvol)
+{
+    constexpr int N = 64, P = N + 1;
+    constexpr long long PLANE = (long long)N * N;
+    using T = double;
+    using TG = TwoPassGeom<N, N, N, T, 1>;
+    const T scale = S > 0 ? T(1) / T(TG::V) : T(1);
+    int lag = 0;
+    const int R = twopass_ring_size(TG::NA, TG::NB, 7, &lag);
+    std::vector<cx<T>> smv((size_t)N * P), ring((size_t)R * TG::V, cx<T>{T(-777.0), T(555.0)});
+    cx<T> *sm = smv.data();
+    const cx<T> *in = (const cx<T> *)vin;
+    cx<T> *out = (cx<T> *)vout;
+    const long long total = (long long)(TG::NA + TG::NB) * nvol;
+    std::vector<long long> cnt_plane(R, 0), cnt_row(R, 0);
+    auto rowaddr = [](int l, int e) { return l * P + e; };
+    auto coladdr = [](int l, int e) { return e * P + l; };
+    for (long long t = 0; t < total; ++t) {
+        const TwoPassItem it = twopass_decode(t, nvol, TG::NA, TG::NB, lag);
+        const int slot = (int)(it.vol % R);
+        const long long round = it.vol / R;
+        cx<T> *sv = ring.data() + slot * TG::V;
+        if (it.plane ? cnt_row[slot] < TG::NB * round : cnt_plane[slot] < TG::NA * (round + 1))
+            g_twopass_violations++;
+        (it.plane ? cnt_plane : cnt_row)[slot]++;
+        for (auto &e : smv) e = {T(12345.0), T(-6789.0)};
+        if (it.plane) {
+            const cx<T> *rows = in + it.vol * TG::V + (long long)it.j * PLANE;
+            for (int r = 0; r < N; ++r)
+                for (int z = 0; z < N; ++z) sm[r * P + z] = rows[(long long)r * N + z];
+            for (int q = 0; q < N * 8; ++q) ct64_stage1<S, T>(sm, N, q, rowaddr);
+            for (int q = 0; q < N * 8; ++q)
+                ct64_stage2<S, T>(sm, N, q, rowaddr, [&](int l, int k, cx<T> v) { sm[rowaddr(l, ct64_slot(k))] = v; });
+            for (int q = 0; q < N * 8; ++q) ct64_stage1<S, T>(sm, N, q, coladdr);
+            cx<T> *dst = sv + (long long)it.j * PLANE;
+            for (int q = 0; q < N * 8; ++q)
+                ct64_stage2<S, T>(sm, N, q, coladdr, [&](int p, int k, cx<T> v) { dst[k * N + ct64_slot(p)] = v; });
+        } else {
+            for (int x = 0; x < N; ++x)
+                for (int z = 0; z < N; ++z) sm[x * P + z] = sv[((long long)x * N + it.j) * N + z];
+            for (int q = 0; q < N * 8; ++q) ct64_stage1<S, T>(sm, N, q, coladdr);
+            cx<T> *gvol = out + it.vol * TG::V + (long long)it.j * N;
+            for (int q = 0; q < N * 8; ++q)
+                ct64_stage2<S, T>(sm, N, q, coladdr, [&](int z, int k, cx<T> v) {
+                    if (S > 0) v = cscale(v, scale);
+                    gvol[k * PLANE + z] = v;
+                });
+        }
+    }
+}
+
 // The split-line TWOPASS variant (SPLIT = true): every pass whose length has a
 // lane split runs split_line_host over whole lines, the host form of the
 // kernel's lane exchange; other axes keep the one-thread-per-line pass.
@@ -386,6 +444,8 @@ typedef void (*emu_fn)(const void *, void *, long long);
 #define EMU_TPP(G)                                                                            \
     {36, 36, 36, 0, -1, 600 + G, 1, &emulate_twopass_pfa<-1, G>},                               \
     {36, 36, 36, 0, +1, 600 + G, 1, &emulate_twopass_pfa<+1, G>}
+#define EMU_TPCT64                                                                            \
+    {64, 64, 64, 0, -1, 701, 1, &emulate_twopass_ct64<-1>}, {64, 64, 64, 0, +1, 701, 1, &emulate_twopass_ct64<+1>}
 #define EMU_TP(N0, N1, N2, T, G)                                                              \
     {N0, N1, N2, sizeof(T) == 8 ? 0 : 1, -1, 300 + G, 1,                                    \
      &emulate_twopass<N0, N1, N2, T, -1, G>},                                                \
@@ -433,7 +493,7 @@ static const EmuEntry kEmu[] = {
     EMU_TPS(36, 36, 36, double, 2), EMU_TPS(36, 36, 36, double, 1), EMU_TPS(36, 36, 36, float, 4),
     EMU_TPS(64, 64, 64, double, 1), EMU_TPS(64, 64, 64, float, 2),  EMU_TPS(36, 36, 64, double, 2),
     EMU_TPR(36, 36, 36, 3), EMU_TPR(36, 36, 36, 2), EMU_TPR(36, 36, 36, 4), EMU_TPRP(36, 36, 36, 3), EMU_TPRP(36, 36, 36, 2), EMU_TPRQ(36, 36, 36, 3),
-    EMU_TPRQ(36, 36, 36, 2), EMU_TPRP(45, 45, 45, 3), EMU_TPRP(6, 9, 5, 3), EMU_TPRQ(6, 9, 5, 3), EMU_TPP(2), EMU_TPP(3), EMU_TPP(4),
+    EMU_TPRQ(36, 36, 36, 2), EMU_TPRP(45, 45, 45, 3), EMU_TPRP(6, 9, 5, 3), EMU_TPRQ(6, 9, 5, 3), EMU_TPP(2), EMU_TPP(3), EMU_TPP(4), EMU_TPCT64,
     EMU_TPR(6, 9, 5, 3),
 };
 

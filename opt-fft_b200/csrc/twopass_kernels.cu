@@ -22,6 +22,7 @@
 // launch, on the error path as well.
 #include <algorithm>
 
+#include "ct64.cuh"
 #include "internal.h"
 #include "pfa36.cuh"
 #include "ptx.cuh"
@@ -781,6 +782,156 @@ __global__ void __launch_bounds__(NT, MINB)
     }
 }
 
+// TWOPASS for 64^3 complex double with every 64-point line split into its
+// 8 x 8 Cooley-Tukey stages (ct64.cuh): one plane or one y-row per item, eight
+// points per thread task, ~85 registers, 24 warps per SM -- where a 64-point
+// line in one thread spills about 1.3 KB.  Rows are held at an odd pitch of 65
+// points (bank-conflict-free for rows and columns) and moved by bulk copies.
+// The z pass runs in place, leaving each row in ct64_slot order; the y pass's
+// second stage stores into the scratch slot at the natural z; the row item's
+// second stage streams the output.  Item control, L2 policies and the slot
+// release as in k_twopass_regs.
+template <int S, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
+    k_twopass_ct64(const cx<double> *__restrict__ in, cx<double> *__restrict__ out, long long nvol,
+                   double scale, int *err, unsigned char *work, int R, int D)
+{
+    pdl_begin();
+    constexpr int N = 64, P = N + 1;
+    using T = double;
+    using TG = TwoPassGeom<N, N, N, T, 1>;
+    static_assert(NT % 32 == 0, "whole warps");
+    constexpr uint32_t ROW_BYTES = (uint32_t)(N * sizeof(cx<T>));
+    constexpr long long PLANE = (long long)N * N;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);
+    __shared__ long long s_t;
+    __shared__ int s_stop;
+    __shared__ __align__(8) uint64_t s_bar;
+    TwoPassCtl *ctl = reinterpret_cast<TwoPassCtl *>(work);
+    cx<T> *ring = reinterpret_cast<cx<T> *>(work + TWOPASS_CTL_BYTES);
+    const int tid = threadIdx.x;
+    const long long total = (long long)(TG::NA + TG::NB) * nvol;
+    uint32_t phase = 0;
+    bool copies_pending = false;
+    long long next = 0;  // thread 0: the ticket taken ahead
+    const uint64_t pol_first = l2_policy_evict_first(), pol_last = l2_policy_evict_last();
+    if (tid == 0) {
+        mbar_init(&s_bar, 1);
+        fence_mbar_init();
+        next = (long long)atomicAdd(&ctl->ticket, 1ull);
+    }
+    auto wait_copies = [&]() {
+        copies_pending = true;
+        const bool ok = mbar_wait_bounded(&s_bar, phase);
+        phase ^= 1u;
+        if (ok) copies_pending = false;
+        return ok;
+    };
+    auto rowaddr = [](int l, int e) { return l * P + e; };  // element e of row l
+    auto coladdr = [](int l, int e) { return e * P + l; };  // element e of column l
+
+    for (;;) {
+        if (tid == 0) {
+            const long long t = next;
+            int stop = t >= total ? 1 : 0;
+            if (!stop) {
+                next = (long long)atomicAdd(&ctl->ticket, 1ull);
+                const TwoPassItem it = twopass_decode(t, nvol, TG::NA, TG::NB, D);
+                // a row item reads its slot: its plane items must be done first
+                const unsigned target = (unsigned)TG::NA * (unsigned)(it.vol / R + 1);
+                if (!it.plane && !wait_counter_geq(&ctl->cnt[it.vol % R], target, &ctl->abort)) stop = 2;
+            }
+            s_t = t;
+            s_stop = stop;
+        }
+        __syncthreads();
+        if (s_stop) break;
+        const TwoPassItem it = twopass_decode(s_t, nvol, TG::NA, TG::NB, D);
+        const int slot = (int)(it.vol % R);
+        cx<T> *sv = ring + (long long)slot * TG::V;
+
+        if (it.plane) {
+            // 1. x-plane j of the input, one bulk copy per y-row (read once: evict_first)
+            if (tid == 0) mbar_arrive_expect_tx(&s_bar, (uint32_t)N * ROW_BYTES);
+            const cx<T> *rows = in + it.vol * TG::V + (long long)it.j * PLANE;
+            for (int r = tid; r < N; r += NT)
+                bulk_g2s_hint(sm + r * P, rows + (long long)r * N, ROW_BYTES, &s_bar, pol_first);
+            // while the rows are in flight: the slot's previous volume must have
+            // been read out before this item's y pass stores into it
+            if (tid == 0) {
+                const unsigned target = (unsigned)TG::NB * (unsigned)(it.vol / R);
+                if (target > 0 && !wait_counter_geq(&ctl->cnt[TWOPASS_RMAX + slot], target, &ctl->abort))
+                    s_stop = 2;
+            }
+            if (!wait_copies()) s_stop = 2;
+            __syncthreads();
+            if (s_stop) break;
+            // 2. z pass along the rows, in place (rows end in ct64_slot order)
+            for (int t = tid; t < N * 8; t += NT) ct64_stage1<S, T>(sm, N, t, rowaddr);
+            __syncthreads();
+            for (int t = tid; t < N * 8; t += NT)
+                ct64_stage2<S, T>(sm, N, t, rowaddr, [&](int l, int k, cx<T> v) { sm[rowaddr(l, ct64_slot(k))] = v; });
+            __syncthreads();
+            // 3. y pass along the columns; column p holds z = ct64_slot(p)
+            for (int t = tid; t < N * 8; t += NT) ct64_stage1<S, T>(sm, N, t, coladdr);
+            __syncthreads();
+            cx<T> *dst = sv + (long long)it.j * PLANE;
+            for (int t = tid; t < N * 8; t += NT)
+                ct64_stage2<S, T>(sm, N, t, coladdr, [&](int p, int k, cx<T> v) {
+                    st_cg_hint(reinterpret_cast<double2 *>(dst + k * N + ct64_slot(p)), make_double2(v.re, v.im),
+                               pol_last);
+                });
+            fence_proxy_async_smem();  // these reads before the next item's bulk copies
+            __syncthreads();  // then one cumulative release publishes every thread's stores
+            if (tid == 0) red_release_gpu_add(&ctl->cnt[slot], 1u);
+        } else {
+            // 1. y-row j of every x-plane of the slot (its plane items are done)
+            if (tid == 0) mbar_arrive_expect_tx(&s_bar, (uint32_t)N * ROW_BYTES);
+            for (int x = tid; x < N; x += NT) {
+                fence_proxy_async_global();  // the acquire above precedes these reads
+                bulk_g2s(sm + x * P, sv + ((long long)x * N + it.j) * N, ROW_BYTES, &s_bar);
+            }
+            if (!wait_copies()) s_stop = 2;
+            __syncthreads();
+            if (s_stop) break;
+            // the slot may be overwritten: its rows are in shared memory
+            if (tid == 0) red_release_gpu_add(&ctl->cnt[TWOPASS_RMAX + slot], 1u);
+            // 2. x pass along the columns (column z), streamed to the output
+            for (int t = tid; t < N * 8; t += NT) ct64_stage1<S, T>(sm, N, t, coladdr);
+            __syncthreads();
+            cx<T> *gvol = out + it.vol * TG::V + (long long)it.j * N;
+            for (int t = tid; t < N * 8; t += NT)
+                ct64_stage2<S, T>(sm, N, t, coladdr, [&](int z, int k, cx<T> v) {
+                    if constexpr (S > 0) v = cscale(v, scale);
+                    store_out(gvol + k * PLANE + z, v);
+                });
+            fence_proxy_async_smem();
+            __syncthreads();
+        }
+    }
+    // a bulk copy that timed out may still land: wait once more (bounded)
+    if (copies_pending) mbar_wait_bounded(&s_bar, phase ^ 1u);
+
+    if (tid == 0 && s_stop == 2) {
+        report_error(err, DEV_ERR_DEP_TIMEOUT);
+        atomicExch(&ctl->abort, 1u);
+    }
+    // The last CTA to leave clears the control block for the next launch.
+    if (tid == 0) {
+        __threadfence();
+        const unsigned prev = atomicAdd(&ctl->done, 1u);
+        if (prev == gridDim.x - 1) {
+            __threadfence();
+            ctl->ticket = 0ull;
+            for (int i = 0; i < 2 * TWOPASS_RMAX; ++i) ctl->cnt[i] = 0u;
+            ctl->abort = 0u;
+            __threadfence();
+            ctl->done = 0u;
+        }
+    }
+}
+
 int twopass_ring(const KernelEntry &e, long long grid, int *lag)
 {
     // The lag covers up to twice the tickets the grid holds at once: kernels
@@ -924,6 +1075,28 @@ static void add_twopass_pfa(std::vector<KernelEntry> &out, const char *name)
     add_twopass_pfa<-1, G, NT, MINB>(out, "twopass 36x36x36 double g" #G " pfa nt" #NT " minb" #MINB); \
     add_twopass_pfa<+1, G, NT, MINB>(out, "twopass 36x36x36 double g" #G " pfa nt" #NT " minb" #MINB)
 
+template <int S, int NT, int MINB>
+static void add_twopass_ct64(std::vector<KernelEntry> &out, const char *name)
+{
+    KernelEntry e;
+    e.n0 = e.n1 = e.n2 = 64;
+    e.precision = FFT3D_B200_C128;
+    e.sign = S;
+    e.family = FAM_TWOPASS;  // same launch arguments and workspace as k_twopass
+    e.alg = 512;
+    e.vpc = 1;
+    e.threads = NT;
+    e.smem = 64 * 65 * (int)sizeof(cx<double>);
+    e.func = (const void *)&k_twopass_ct64<S, NT, MINB>;
+    e.name = name;
+    out.push_back(e);
+}
+
+// 64^3 complex double, lines split into their 8 x 8 stages: "ct" in the name.
+#define FFT3D_TWOPASS_CT64(NT, MINB)                                                               \
+    add_twopass_ct64<-1, NT, MINB>(out, "twopass 64x64x64 double g1 ct nt" #NT " minb" #MINB);    \
+    add_twopass_ct64<+1, NT, MINB>(out, "twopass 64x64x64 double g1 ct nt" #NT " minb" #MINB)
+
 // Rows moved by bulk copies (complex double, row-major layouts): "bulk" in the name.
 #define FFT3D_TWOPASS_BULK(N0, N1, N2, G, NT, MINB)                                              \
     add_twopass<N0, N1, N2, double, -1, G, NT, MINB, false, true>(                               \
@@ -957,6 +1130,10 @@ void register_twopass_kernels(std::vector<KernelEntry> &out)
     FFT3D_TWOPASS_BULKQ(36, 36, 36, 3, 128, 3);
     FFT3D_TWOPASS_BULKQ(36, 36, 36, 2, 96, 4);
     FFT3D_TWOPASS_BULKP(45, 45, 45, 3, 160, 2);
+    // 64-point lines as 8 x 8 stages: one plane or y-row per item, 24 warps per SM
+    FFT3D_TWOPASS_CT64(256, 3);
+    FFT3D_TWOPASS_CT64(384, 2);
+    FFT3D_TWOPASS_CT64(128, 3);
     // 36-point lines as 4 x 9 stages: ~85 registers, 24 warps per SM
     FFT3D_TWOPASS_PFA36(3, 256, 3);
     FFT3D_TWOPASS_PFA36(2, 256, 4);

@@ -173,6 +173,24 @@ def test_twopass_pfa36_stages(hostcheck, g, nvol, sign):
     assert oracle.rel_error_per_volume(got, want).max() < C128_TOL
 
 
+@pytest.mark.parametrize("nvol", [1, 3])
+@pytest.mark.parametrize("sign", [-1, +1])
+def test_twopass_ct64_stages(hostcheck, nvol, sign):
+    """64^3 TWOPASS with every line split into its 8 x 8 Cooley-Tukey stages
+    (alg = 701): the twiddles and index maps of ct64.cuh, the digit-reversed
+    in-place z pass and the natural-order stores, in ticket order with the
+    dependency check."""
+    import ctypes
+    hostcheck.hostcheck_twopass_violations.restype = ctypes.c_longlong
+    hostcheck.hostcheck_twopass_violations()
+    rng = np.random.default_rng(9000 + nvol)
+    x = field(rng, (nvol, 64, 64, 64), dist="normal")
+    got = run(hostcheck, x, (64, 64, 64), 0, sign, 701, 1)
+    assert hostcheck.hostcheck_twopass_violations() == 0
+    want = oracle.fft3d(x) if sign < 0 else oracle.ifft3d(x)
+    assert oracle.rel_error_per_volume(got, want).max() < C128_TOL
+
+
 SPLIT = [((36, 36, 36), 0, 2, 11), ((36, 36, 36), 0, 1, 3), ((36, 36, 36), 1, 4, 5),
          ((64, 64, 64), 0, 1, 3), ((64, 64, 64), 1, 2, 2), ((36, 36, 64), 0, 2, 4)]
 

@@ -61,55 +61,68 @@ static void add_direct(std::vector<KernelEntry> &out, const char *name)
     add_direct<N0, N1, N2, T, +1, ALG, VPC, NT, MINB>(                                        \
         out, "direct " #N0 "x" #N1 "x" #N2 " " #T " alg" #ALG " vpc" #VPC " nt" #NT " minb" #MINB)
 
-// DIRECT, pipelined across volumes ("directp"): persistent CTAs, one volume
-// at a time.  Each thread owns ROWS/NT z-lines; right after the z pass has put
-// the current volume into shared memory, the thread starts loading its lines
-// of the CTA's next volume into the same registers, and only uses them after
-// the current volume's y and x passes -- so a volume that fills an SM's shared
-// memory alone (16x16x32 complex double, 131 KB) still overlaps its HBM reads
-// with arithmetic.
-template <class G, int S, int NT>
-__global__ void __launch_bounds__(NT, 1)
+// DIRECT, pipelined across items ("directp"): persistent CTAs, one item of
+// VPC volumes at a time.  Each thread owns z-lines r = q*NT + tid of the item;
+// right after the z pass has put the current item into shared memory, the
+// thread starts loading its lines of the CTA's next item into the same
+// registers, and only uses them after the current item's y and x passes -- so
+// the HBM reads of one item overlap the arithmetic of the previous one, even
+// when a single item fills an SM's shared memory (16x16x32 complex double,
+// 131 KB).
+template <class G, int S, int VPC, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB)
     k_direct_pipe(const cx<typename G::T> *__restrict__ in, cx<typename G::T> *__restrict__ out,
                   long long nvol, typename G::T scale, int *err)
 {
     pdl_begin();
     (void)err;
     using T = typename G::T;
-    static_assert(G::ROWS % NT == 0, "whole z-lines per thread");
-    constexpr int RPT = G::ROWS / NT;
+    constexpr int RPT = (VPC * G::ROWS + NT - 1) / NT;  // z-lines per thread
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);
     const int tid = threadIdx.x;
-    long long vol = blockIdx.x;
-    if (vol >= nvol) return;
-    cx<T> v[RPT][G::N2];
-    auto load = [&](long long w) {
-        const cx<T> *g = in + w * G::V;
-#pragma unroll
-        for (int q = 0; q < RPT; ++q)
-#pragma unroll
-            for (int j = 0; j < G::N2; ++j) v[q][j] = load_in(g + (long long)(q * NT + tid) * G::N2 + j);
+    const long long nitems = (nvol + VPC - 1) / VPC;
+    long long item = blockIdx.x;
+    if (item >= nitems) return;
+    auto vols = [&](long long it) {
+        const long long left = nvol - it * VPC;
+        return left < VPC ? (int)left : VPC;
     };
-    load(vol);
-    for (; vol < nvol; vol += gridDim.x) {
+    cx<T> v[RPT][G::N2];
+    auto load = [&](long long it) {
+        const cx<T> *g = in + it * VPC * G::V;
+        const int nr = vols(it) * G::ROWS;
 #pragma unroll
         for (int q = 0; q < RPT; ++q) {
-            dft<G::N2, S, T>(v[q]);
+            const int r = q * NT + tid;
+            if (r < nr)
 #pragma unroll
-            for (int j = 0; j < G::N2; ++j) sm[G::off(q * NT + tid, j)] = v[q][j];
+                for (int j = 0; j < G::N2; ++j) v[q][j] = load_in(g + (long long)r * G::N2 + j);
+        }
+    };
+    load(item);
+    for (; item < nitems; item += gridDim.x) {
+        const int nv = vols(item);
+#pragma unroll
+        for (int q = 0; q < RPT; ++q) {
+            const int r = q * NT + tid;
+            if (r < nv * G::ROWS) {
+                dft<G::N2, S, T>(v[q]);
+#pragma unroll
+                for (int j = 0; j < G::N2; ++j) sm[G::off(r, j)] = v[q][j];
+            }
         }
         __syncthreads();
-        if (vol + gridDim.x < nvol) load(vol + gridDim.x);  // consumed at the next z pass
-        for (int l = tid; l < G::N0 * G::N2; l += NT) pass_y<G, S, ALG_DEFAULT>(sm, l);
+        if (item + gridDim.x < nitems) load(item + gridDim.x);  // consumed at the next z pass
+        for (int l = tid; l < nv * G::N0 * G::N2; l += NT) pass_y<G, S, ALG_DEFAULT>(sm, l);
         __syncthreads();
-        cx<T> *gout = out + vol * G::V;
-        for (int l = tid; l < G::N1 * G::N2; l += NT) pass_x_out<G, S, ALG_DEFAULT>(sm, l, gout, scale);
+        cx<T> *gout = out + item * VPC * G::V;
+        for (int l = tid; l < nv * G::N1 * G::N2; l += NT) pass_x_out<G, S, ALG_DEFAULT>(sm, l, gout, scale);
         __syncthreads();  // shared memory is rewritten by the next z pass
     }
 }
 
-template <int N0, int N1, int N2, typename T, int S, int NT>
+template <int N0, int N1, int N2, typename T, int S, int VPC, int NT, int MINB>
 static void add_direct_pipe(std::vector<KernelEntry> &out, const char *name)
 {
     using G = Geom<N0, N1, N2, T>;
@@ -119,19 +132,21 @@ static void add_direct_pipe(std::vector<KernelEntry> &out, const char *name)
     e.n2 = N2;
     e.precision = sizeof(T) == 8 ? FFT3D_B200_C128 : FFT3D_B200_C64;
     e.sign = S;
-    e.family = FAM_STREAM;  // persistent launch: (in, out, nvol, scale, err)
+    e.family = FAM_STREAM;  // persistent launch over items of vpc volumes: (in, out, nvol, scale, err)
     e.alg = 0;
-    e.vpc = 1;
+    e.vpc = VPC;
     e.threads = NT;
-    e.smem = G::PV * G::EB;
-    e.func = (const void *)&k_direct_pipe<G, S, NT>;
+    e.smem = VPC * G::PV * G::EB;
+    e.func = (const void *)&k_direct_pipe<G, S, VPC, NT, MINB>;
     e.name = name;
     out.push_back(e);
 }
 
-#define FFT3D_DIRECT_PIPE(N0, N1, N2, T, NT)                                                       \
-    add_direct_pipe<N0, N1, N2, T, -1, NT>(out, "directp " #N0 "x" #N1 "x" #N2 " " #T " nt" #NT);    \
-    add_direct_pipe<N0, N1, N2, T, +1, NT>(out, "directp " #N0 "x" #N1 "x" #N2 " " #T " nt" #NT)
+#define FFT3D_DIRECT_PIPE(N0, N1, N2, T, VPC, NT, MINB)                                            \
+    add_direct_pipe<N0, N1, N2, T, -1, VPC, NT, MINB>(                                             \
+        out, "directp " #N0 "x" #N1 "x" #N2 " " #T " vpc" #VPC " nt" #NT " minb" #MINB);           \
+    add_direct_pipe<N0, N1, N2, T, +1, VPC, NT, MINB>(                                             \
+        out, "directp " #N0 "x" #N1 "x" #N2 " " #T " vpc" #VPC " nt" #NT " minb" #MINB)
 
 void register_direct_kernels(std::vector<KernelEntry> &out)
 {
@@ -147,7 +162,12 @@ void register_direct_kernels(std::vector<KernelEntry> &out)
     FFT3D_DIRECT(24, 24, 24, double, 0, 1, 288, 1);
     FFT3D_DIRECT(8, 8, 16, double, 0, 2, 256, 2);
     FFT3D_DIRECT(16, 16, 32, double, 0, 1, 256, 1);
-    FFT3D_DIRECT_PIPE(16, 16, 32, double, 256);
+    // pipelined through registers
+    FFT3D_DIRECT_PIPE(16, 16, 32, double, 1, 256, 1);
+    FFT3D_DIRECT_PIPE(16, 16, 16, double, 1, 256, 1);
+    FFT3D_DIRECT_PIPE(17, 17, 17, double, 1, 320, 1);
+    FFT3D_DIRECT_PIPE(12, 12, 12, double, 2, 288, 1);
+    FFT3D_DIRECT_PIPE(8, 8, 8, double, 4, 256, 2);
     // complex float
     FFT3D_DIRECT(6, 6, 6, float, 0, 16, 576, 2);
     FFT3D_DIRECT(8, 8, 8, float, 0, 8, 512, 2);
@@ -160,6 +180,16 @@ void register_direct_kernels(std::vector<KernelEntry> &out)
     FFT3D_DIRECT(24, 24, 24, float, 0, 1, 576, 1);
     FFT3D_DIRECT(8, 8, 16, float, 0, 4, 512, 2);
     FFT3D_DIRECT(16, 16, 32, float, 0, 1, 512, 1);
+    // pipelined through registers
+    FFT3D_DIRECT_PIPE(6, 6, 6, float, 16, 576, 1);
+    FFT3D_DIRECT_PIPE(8, 8, 8, float, 4, 256, 3);
+    FFT3D_DIRECT_PIPE(8, 8, 8, float, 8, 512, 2);
+    FFT3D_DIRECT_PIPE(12, 12, 12, float, 2, 288, 3);
+    FFT3D_DIRECT_PIPE(16, 16, 16, float, 1, 256, 3);
+    FFT3D_DIRECT_PIPE(17, 17, 17, float, 1, 320, 2);
+    FFT3D_DIRECT_PIPE(24, 24, 24, float, 1, 576, 1);
+    FFT3D_DIRECT_PIPE(8, 8, 16, float, 8, 512, 2);
+    FFT3D_DIRECT_PIPE(16, 16, 32, float, 1, 512, 1);
 }
 
 }  // namespace fft3d

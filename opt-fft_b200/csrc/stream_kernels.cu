@@ -95,8 +95,13 @@ __global__ void __launch_bounds__(NT, MINB)
 
     // Issue the load of `item` into stage s.  For BULK, returns with the copy in
     // flight (or, for an unaligned item, done by the threads and arrived).
+    // Inverse transforms walk their items from the last to the first: after a
+    // forward transform (which walks them in order) the volumes it wrote last
+    // are still in L2 when the inverse starts, and are read first.
+    auto phys = [&](long long item) { return S > 0 ? nitems - 1 - item : item; };
+    const uint64_t pol_first = l2_policy_evict_first();
     auto issue = [&](long long item, int s) {
-        const long long v0 = item * VPC;
+        const long long v0 = phys(item) * VPC;
         const int nv = (int)((nvol - v0) < VPC ? (nvol - v0) : VPC);
         const cx<T> *gin = in + v0 * G::V;
         const int nel = nv * G::V;
@@ -104,9 +109,9 @@ __global__ void __launch_bounds__(NT, MINB)
             const uint32_t bytes = (uint32_t)nel * (uint32_t)G::EB;
             const bool aligned = ((((uintptr_t)gin) | bytes) & 15u) == 0;
             if (aligned) {
-                if (tid == 0) {
+                if (tid == 0) {  // read once: keep L2 for the output
                     mbar_arrive_expect_tx(&bar[s], bytes);
-                    bulk_g2s(stage(s), gin, bytes, &bar[s]);
+                    bulk_g2s_hint(stage(s), gin, bytes, &bar[s], pol_first);
                 }
             } else {
                 load_lsu<G>(stage(s), gin, nel, tid, NT);
@@ -139,7 +144,7 @@ __global__ void __launch_bounds__(NT, MINB)
         __syncthreads();
         if (s_abort) break;
 
-        const long long v0 = item * VPC;
+        const long long v0 = phys(item) * VPC;
         const int nv = (int)((nvol - v0) < VPC ? (nvol - v0) : VPC);
         cx<T> *sm = stage(cur);
         for (int r = tid; r < nv * G::ROWS; r += NT) pass_z<G, S, ALG>(sm, r);
@@ -147,7 +152,8 @@ __global__ void __launch_bounds__(NT, MINB)
         for (int l = tid; l < nv * G::N0 * G::N2; l += NT) pass_y<G, S, ALG>(sm, l);
         __syncthreads();
         cx<T> *gout = out + v0 * G::V;
-        for (int l = tid; l < nv * G::N1 * G::N2; l += NT) pass_x_out<G, S, ALG>(sm, l, gout, scale);
+        // plain stores: a following transform of this output finds its last part in L2
+        for (int l = tid; l < nv * G::N1 * G::N2; l += NT) pass_x_out<G, S, ALG, true>(sm, l, gout, scale);
         if constexpr (LOADER == LOADER_BULK) fence_proxy_async_smem();
         __syncthreads();
     }

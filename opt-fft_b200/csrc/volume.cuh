@@ -116,7 +116,9 @@ FFT_HD cx<T> load_in(const cx<T> *p)
 #endif
 }
 
-template <class G, int S, int ALG>
+// KEEP: plain stores instead of streaming (evict-first) ones, for outputs that
+// a following transform may still find in L2.
+template <class G, int S, int ALG, bool KEEP = false>
 FFT_HD void pass_x_out(const cx<typename G::T> *sm, int l, cx<typename G::T> *gout,
                        typename G::T scale)
 {
@@ -134,7 +136,8 @@ FFT_HD void pass_x_out(const cx<typename G::T> *sm, int l, cx<typename G::T> *go
     for (int j = 0; j < G::N0; ++j) {
         cx<T> r = v[j];
         if constexpr (S > 0) r = cscale(r, scale);
-        store_out(o + j * (G::N1 * G::N2), r);
+        if constexpr (KEEP) o[j * (G::N1 * G::N2)] = r;
+        else store_out(o + j * (G::N1 * G::N2), r);
     }
 }
 

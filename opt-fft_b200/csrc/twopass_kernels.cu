@@ -1,9 +1,9 @@
 // twopass_kernels.cu -- kernel family TWOPASS: volumes larger than one SM's
-// shared memory (36^3 complex double is 746 KB, 16x16x32 is 262 KB), in plane
-// and row items through an L2-resident scratch ring (twopass.cuh).
+// shared memory (36^3 complex double is 746 KB, 64^3 is 4 MB), in plane and
+// row items through an L2-resident scratch ring (twopass.cuh).
 //
-// Persistent CTAs take one ticket at a time.  A plane item copies its G
-// contiguous x-planes into shared memory with cp.async, runs the z and y
+// Persistent CTAs take tickets.  A plane item copies its G contiguous x-planes
+// into shared memory (cp.async, or one bulk copy per row), runs the z and y
 // passes, and writes the planes to the volume's scratch slot with L2-only
 // stores; a row item reads its G y-rows of all planes back with L2-only loads
 // (never through L1, which is not coherent with other SMs' stores), runs the

@@ -181,10 +181,10 @@ static void emulate_twopass(const void *vin, void *vout, long long nvol)
 // and copied by rows; x pass loaded straight from the slot or from rows
 // gathered into the row layout (XBULK).  Same tickets, ring and dependency
 // checks as emulate_twopass.
-template <int N0, int N1, int N2, typename T, int S, int G, bool XBULK, bool YDIRECT>
+template <int N0, int N1, int N2, typename T, int S, int G, bool XBULK, bool YDIRECT, int PITCH = 0>
 static void emulate_twopass_regs(const void *vin, void *vout, long long nvol)
 {
-    using TG = TwoPassGeom<N0, N1, N2, T, G>;
+    using TG = TwoPassGeom<N0, N1, N2, T, G, PITCH>;
     using XG = typename TG::XG;
     using YG = typename TG::YG;
     const T scale = S > 0 ? T(1) / T(TG::V) : T(1);
@@ -441,6 +441,9 @@ typedef void (*emu_fn)(const void *, void *, long long);
 #define EMU_TPR(N0, N1, N2, G) EMU_TPR_(N0, N1, N2, G, 500, false, true)
 #define EMU_TPRP(N0, N1, N2, G) EMU_TPR_(N0, N1, N2, G, 520, true, false)
 #define EMU_TPRQ(N0, N1, N2, G) EMU_TPR_(N0, N1, N2, G, 540, true, true)
+#define EMU_TPRQF(G)                                                                          \
+    {36, 36, 36, 1, -1, 540 + G, 1, &emulate_twopass_regs<36, 36, 36, float, -1, G, true, true, 38>},  \
+    {36, 36, 36, 1, +1, 540 + G, 1, &emulate_twopass_regs<36, 36, 36, float, +1, G, true, true, 38>}
 #define EMU_TPP(G)                                                                            \
     {36, 36, 36, 0, -1, 600 + G, 1, &emulate_twopass_pfa<-1, G>},                               \
     {36, 36, 36, 0, +1, 600 + G, 1, &emulate_twopass_pfa<+1, G>}
@@ -493,7 +496,7 @@ static const EmuEntry kEmu[] = {
     EMU_TPS(36, 36, 36, double, 2), EMU_TPS(36, 36, 36, double, 1), EMU_TPS(36, 36, 36, float, 4),
     EMU_TPS(64, 64, 64, double, 1), EMU_TPS(64, 64, 64, float, 2),  EMU_TPS(36, 36, 64, double, 2),
     EMU_TPR(36, 36, 36, 3), EMU_TPR(36, 36, 36, 2), EMU_TPR(36, 36, 36, 4), EMU_TPRP(36, 36, 36, 3), EMU_TPRP(36, 36, 36, 2), EMU_TPRQ(36, 36, 36, 3),
-    EMU_TPRQ(36, 36, 36, 2), EMU_TPRP(45, 45, 45, 3), EMU_TPRP(6, 9, 5, 3), EMU_TPRQ(6, 9, 5, 3), EMU_TPP(2), EMU_TPP(3), EMU_TPP(4), EMU_TPCT64,
+    EMU_TPRQ(36, 36, 36, 2), EMU_TPRP(45, 45, 45, 3), EMU_TPRP(6, 9, 5, 3), EMU_TPRQ(6, 9, 5, 3), EMU_TPRQF(3), EMU_TPRQF(2), EMU_TPRQF(4), EMU_TPP(2), EMU_TPP(3), EMU_TPP(4), EMU_TPCT64,
     EMU_TPR(6, 9, 5, 3),
 };
 

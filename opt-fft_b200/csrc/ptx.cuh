@@ -163,10 +163,17 @@ __device__ __forceinline__ void bulk_g2s_hint(void *dst, const void *src, uint32
         : "memory");
 }
 
-// 16-byte L2-only store with an L2 cache policy.
+// L2-only stores of one complex value with an L2 cache policy.
 __device__ __forceinline__ void st_cg_hint(double2 *p, double2 v, uint64_t policy)
 {
     asm volatile("st.global.cg.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;" ::"l"(p), "d"(v.x), "d"(v.y),
+                 "l"(policy)
+                 : "memory");
+}
+
+__device__ __forceinline__ void st_cg_hint(float2 *p, float2 v, uint64_t policy)
+{
+    asm volatile("st.global.cg.L2::cache_hint.v2.f32 [%0], {%1, %2}, %3;" ::"l"(p), "f"(v.x), "f"(v.y),
                  "l"(policy)
                  : "memory");
 }

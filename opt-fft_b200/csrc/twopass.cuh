@@ -22,11 +22,11 @@
 
 namespace fft3d {
 
-template <int N0, int N1, int N2, typename T, int G>
+template <int N0, int N1, int N2, typename T, int G, int PITCH = 0>
 struct TwoPassGeom {
     static_assert(N0 % G == 0 && N1 % G == 0, "planes and rows per item must divide n0, n1");
-    using XG = Geom<G, N1, N2, T>;   // plane item: G planes of N1 x N2
-    using YG = Geom<N0, G, N2, T>;   // row item: G rows (y) of all N0 planes
+    using XG = Geom<G, N1, N2, T, PITCH>;   // plane item: G planes of N1 x N2
+    using YG = Geom<N0, G, N2, T, PITCH>;   // row item: G rows (y) of all N0 planes
     static constexpr int N1F = N1;  // full y extent
     static constexpr int NA = N0 / G;
     static constexpr int NB = N1 / G;

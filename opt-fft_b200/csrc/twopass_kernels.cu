@@ -474,18 +474,19 @@ __global__ void __launch_bounds__(NT, MINB)
 // (L2-only loads, a warp reading contiguous ranges; no shared memory at all,
 // "regs") or gather their rows by bulk copies first (XBULK, "bulkp"/"bulkq").
 template <int N0, int N1, int N2, int S, int G, int NT, int MINB, bool XBULK = false,
-          bool YDIRECT = true, bool HINT = false>
+          bool YDIRECT = true, bool HINT = false, typename T = double, int PITCH = 0>
 __global__ void __launch_bounds__(NT, MINB)
-    k_twopass_regs(const cx<double> *__restrict__ in, cx<double> *__restrict__ out, long long nvol,
-                   double scale, int *err, unsigned char *work, int R, int D)
+    k_twopass_regs(const cx<T> *__restrict__ in, cx<T> *__restrict__ out, long long nvol, T scale,
+                   int *err, unsigned char *work, int R, int D)
 {
     pdl_begin();
-    using T = double;
-    using TG = TwoPassGeom<N0, N1, N2, T, G>;
+    using TG = TwoPassGeom<N0, N1, N2, T, G, PITCH>;
     using XG = typename TG::XG;
     using YG = typename TG::YG;
     static_assert(XG::POL != 2 && YG::POL != 2 && NT % 32 == 0, "row-major layouts, whole warps");
     constexpr uint32_t ROW_BYTES = (uint32_t)(N2 * sizeof(cx<T>));
+    static_assert(ROW_BYTES % 16 == 0 && (XG::P2 * XG::EB) % 16 == 0,
+                  "bulk row copies: 16-byte rows at 16-byte aligned shared-memory starts");
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);
     __shared__ long long s_t;
@@ -569,9 +570,14 @@ __global__ void __launch_bounds__(NT, MINB)
 #pragma unroll
                     for (int j = 0; j < N1; ++j) v[j] = sm[XG::off(g * N1 + j, z)];
                     dft<N1, S, T>(v);
-                    double2 *o = reinterpret_cast<double2 *>(sv + (long long)(it.j * G + g) * N1 * N2 + z);
+                    cx<T> *o = sv + (long long)(it.j * G + g) * N1 * N2 + z;
 #pragma unroll
-                    for (int j = 0; j < N1; ++j) st_cg_hint(o + j * N2, make_double2(v[j].re, v[j].im), pol_last);
+                    for (int j = 0; j < N1; ++j) {
+                        if constexpr (sizeof(T) == 8)
+                            st_cg_hint(reinterpret_cast<double2 *>(o + j * N2), make_double2(v[j].re, v[j].im), pol_last);
+                        else
+                            st_cg_hint(reinterpret_cast<float2 *>(o + j * N2), make_float2(v[j].re, v[j].im), pol_last);
+                    }
                 }
             } else if constexpr (YDIRECT) {
                 for (int l = tid; l < G * N2; l += NT) pass_y_store_l2<XG, S>(sm, l, sv, it.j * G);
@@ -1005,16 +1011,16 @@ static void add_twopass_pipe(std::vector<KernelEntry> &out, const char *name)
 }
 
 template <int N0, int N1, int N2, int S, int G, int NT, int MINB, bool XBULK = false, bool YDIRECT = true,
-          bool HINT = false>
+          bool HINT = false, typename T = double, int PITCH = 0>
 static void add_twopass_regs(std::vector<KernelEntry> &out, const char *name)
 {
-    using TG = TwoPassGeom<N0, N1, N2, double, G>;
+    using TG = TwoPassGeom<N0, N1, N2, T, G, PITCH>;
     using XG = typename TG::XG;
     KernelEntry e;
     e.n0 = N0;
     e.n1 = N1;
     e.n2 = N2;
-    e.precision = FFT3D_B200_C128;
+    e.precision = sizeof(T) == 8 ? FFT3D_B200_C128 : FFT3D_B200_C64;
     e.sign = S;
     e.family = FAM_TWOPASS;  // same launch arguments and workspace as k_twopass
     e.alg = 8 + (XBULK ? 32 : 0) + (YDIRECT ? 0 : 64) + (HINT ? 128 : 0);
@@ -1022,7 +1028,7 @@ static void add_twopass_regs(std::vector<KernelEntry> &out, const char *name)
     e.threads = NT;
     // plane items only, unless row items gather their rows into shared memory too
     e.smem = XBULK ? TG::SMEM : ((XG::PV * XG::EB) + 127) / 128 * 128;
-    e.func = (const void *)&k_twopass_regs<N0, N1, N2, S, G, NT, MINB, XBULK, YDIRECT, HINT>;
+    e.func = (const void *)&k_twopass_regs<N0, N1, N2, S, G, NT, MINB, XBULK, YDIRECT, HINT, T, PITCH>;
     e.name = name;
     out.push_back(e);
 }
@@ -1047,6 +1053,13 @@ static void add_twopass_regs(std::vector<KernelEntry> &out, const char *name)
         out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G " bulkqh nt" #NT " minb" #MINB);      \
     add_twopass_regs<N0, N1, N2, +1, G, NT, MINB, true, true, true>(                             \
         out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G " bulkqh nt" #NT " minb" #MINB)
+// bulkqh for complex float at an explicit even row pitch (bulk rows need
+// 16-byte aligned shared-memory starts): "bulkqh" with "float" in the name.
+#define FFT3D_TWOPASS_BULKQH_F(N0, N1, N2, G, NT, MINB, PITCH)                                    \
+    add_twopass_regs<N0, N1, N2, -1, G, NT, MINB, true, true, true, float, PITCH>(                \
+        out, "twopass " #N0 "x" #N1 "x" #N2 " float g" #G " bulkqh nt" #NT " minb" #MINB);        \
+    add_twopass_regs<N0, N1, N2, +1, G, NT, MINB, true, true, true, float, PITCH>(                \
+        out, "twopass " #N0 "x" #N1 "x" #N2 " float g" #G " bulkqh nt" #NT " minb" #MINB)
 #define FFT3D_TWOPASS_BULKQ(N0, N1, N2, G, NT, MINB)                                             \
     add_twopass_regs<N0, N1, N2, -1, G, NT, MINB, true, true>(                                   \
         out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G " bulkq nt" #NT " minb" #MINB);       \
@@ -1122,6 +1135,9 @@ void register_twopass_kernels(std::vector<KernelEntry> &out)
 {
     // lean control: next ticket taken ahead, dependency waited at the top
     FFT3D_TWOPASS_BULKQH(36, 36, 36, 3, 128, 3);
+    FFT3D_TWOPASS_BULKQH_F(36, 36, 36, 3, 128, 5, 38);
+    FFT3D_TWOPASS_BULKQH_F(36, 36, 36, 2, 96, 6, 38);
+    FFT3D_TWOPASS_BULKQH_F(36, 36, 36, 4, 160, 3, 38);
     FFT3D_TWOPASS_BULKQH(45, 45, 45, 3, 160, 2);
     FFT3D_TWOPASS_BULKQH(45, 45, 45, 5, 256, 1);
     FFT3D_TWOPASS_BULKQH(36, 36, 36, 2, 96, 4);

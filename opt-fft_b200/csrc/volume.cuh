@@ -19,7 +19,9 @@
 
 namespace fft3d {
 
-template <int N0_, int N1_, int N2_, typename T_>
+//   PITCH > 0 overrides the policy with a plain row pitch (for rows that bulk
+//   copies move: their shared-memory start must be 16-byte aligned).
+template <int N0_, int N1_, int N2_, typename T_, int PITCH = 0>
 struct Geom {
     using T = T_;
     static constexpr int N0 = N0_, N1 = N1_, N2 = N2_;
@@ -27,8 +29,9 @@ struct Geom {
     static constexpr int ROWS = N0 * N1;
     static constexpr int EB = 2 * (int)sizeof(T);
     static constexpr int GROUP = (EB == 16) ? 8 : 16;
-    static constexpr int POL = (N2 % 2 == 1) ? 0 : ((N2 % GROUP == 0) ? 2 : 1);
-    static constexpr int P2 = (POL == 1) ? N2 + 1 : N2;
+    static_assert(PITCH == 0 || PITCH >= N2, "row pitch below the row length");
+    static constexpr int POL = PITCH > 0 ? 1 : (N2 % 2 == 1) ? 0 : ((N2 % GROUP == 0) ? 2 : 1);
+    static constexpr int P2 = PITCH > 0 ? PITCH : (POL == 1) ? N2 + 1 : N2;
     static constexpr int PV = ROWS * P2;  // shared-memory elements per volume
 
     FFT_HD static int off(int r, int z)

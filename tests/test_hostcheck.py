@@ -131,6 +131,25 @@ REGS = [((36, 36, 36), 500, 3, 7), ((36, 36, 36), 500, 2, 11), ((36, 36, 36), 50
         ((6, 9, 5), 500, 3, 41), ((36, 36, 36), 520, 3, 7), ((36, 36, 36), 520, 2, 5),
         ((36, 36, 36), 540, 3, 6), ((36, 36, 36), 540, 2, 3), ((45, 45, 45), 520, 3, 3),
         ((6, 9, 5), 520, 3, 41), ((6, 9, 5), 540, 3, 41)]
+# complex float at row pitch 38 (bulk rows): (shape, alg base, G, batch)
+REGS_F = [((36, 36, 36), 540, 3, 7), ((36, 36, 36), 540, 2, 5), ((36, 36, 36), 540, 4, 3)]
+
+
+@pytest.mark.parametrize("shape,base,g,nvol", REGS_F, ids=[f"{t[0]}-g{t[2]}-b{t[3]}" for t in REGS_F])
+@pytest.mark.parametrize("sign", [-1, +1])
+def test_twopass_lean_control_complex64(hostcheck, shape, base, g, nvol, sign):
+    """The lean-control TWOPASS kernel in complex float with its explicit row
+    pitch of 38 points (16-byte aligned rows for the bulk copies)."""
+    import ctypes
+    hostcheck.hostcheck_twopass_violations.restype = ctypes.c_longlong
+    hostcheck.hostcheck_twopass_violations()
+    rng = np.random.default_rng(7100 + g + nvol)
+    x = field(rng, (nvol,) + shape, dist="normal", dtype=np.complex64)
+    got = run(hostcheck, x, shape, 1, sign, base + g, 1)
+    assert hostcheck.hostcheck_twopass_violations() == 0
+    x64 = x.astype(np.complex128)
+    want = oracle.fft3d(x64) if sign < 0 else oracle.ifft3d(x64)
+    assert oracle.rel_error_per_volume(got, want).max() < C64_TOL
 
 
 @pytest.mark.parametrize("shape,base,g,nvol", REGS,

@@ -301,12 +301,11 @@ static void emulate_twopass_pfa(const void *vin, void *vout, long long nvol)
 // order), y pass stored into the slot at the natural z, x pass streamed out;
 // every stage-1 task of a pass before any stage-2 task, as the kernel's
 // barrier orders them.  Tickets, ring and dependency checks as emulate_twopass.
-template <int S>
+template <int S, typename T = double>
 static void emulate_twopass_ct64(const void *vin, void *vout, long long nvol)
 {
-    constexpr int N = 64, P = N + 1;
+    constexpr int N = 64, P = sizeof(T) == 8 ? N + 1 : N + 2;
     constexpr long long PLANE = (long long)N * N;
-    using T = double;
     using TG = TwoPassGeom<N, N, N, T, 1>;
     const T scale = S > 0 ? T(1) / T(TG::V) : T(1);
     int lag = 0;
@@ -448,7 +447,9 @@ typedef void (*emu_fn)(const void *, void *, long long);
     {36, 36, 36, 0, -1, 600 + G, 1, &emulate_twopass_pfa<-1, G>},                               \
     {36, 36, 36, 0, +1, 600 + G, 1, &emulate_twopass_pfa<+1, G>}
 #define EMU_TPCT64                                                                            \
-    {64, 64, 64, 0, -1, 701, 1, &emulate_twopass_ct64<-1>}, {64, 64, 64, 0, +1, 701, 1, &emulate_twopass_ct64<+1>}
+    {64, 64, 64, 0, -1, 701, 1, &emulate_twopass_ct64<-1>}, {64, 64, 64, 0, +1, 701, 1, &emulate_twopass_ct64<+1>}, \
+    {64, 64, 64, 1, -1, 701, 1, &emulate_twopass_ct64<-1, float>},                                \
+    {64, 64, 64, 1, +1, 701, 1, &emulate_twopass_ct64<+1, float>}
 #define EMU_TP(N0, N1, N2, T, G)                                                              \
     {N0, N1, N2, sizeof(T) == 8 ? 0 : 1, -1, 300 + G, 1,                                    \
      &emulate_twopass<N0, N1, N2, T, -1, G>},                                                \

@@ -797,14 +797,15 @@ __global__ void __launch_bounds__(NT, MINB)
 // second stage stores into the scratch slot at the natural z; the row item's
 // second stage streams the output.  Item control, L2 policies and the slot
 // release as in k_twopass_regs.
-template <int S, int NT, int MINB>
+template <int S, int NT, int MINB, typename T = double>
 __global__ void __launch_bounds__(NT, MINB)
-    k_twopass_ct64(const cx<double> *__restrict__ in, cx<double> *__restrict__ out, long long nvol,
-                   double scale, int *err, unsigned char *work, int R, int D)
+    k_twopass_ct64(const cx<T> *__restrict__ in, cx<T> *__restrict__ out, long long nvol, T scale,
+                   int *err, unsigned char *work, int R, int D)
 {
     pdl_begin();
-    constexpr int N = 64, P = N + 1;
-    using T = double;
+    // row pitch: odd for 16-byte points; 66 for 8-byte points, whose rows must
+    // still start 16-byte aligned for the bulk copies
+    constexpr int N = 64, P = sizeof(T) == 8 ? N + 1 : N + 2;
     using TG = TwoPassGeom<N, N, N, T, 1>;
     static_assert(NT % 32 == 0, "whole warps");
     constexpr uint32_t ROW_BYTES = (uint32_t)(N * sizeof(cx<T>));
@@ -885,8 +886,11 @@ __global__ void __launch_bounds__(NT, MINB)
             cx<T> *dst = sv + (long long)it.j * PLANE;
             for (int t = tid; t < N * 8; t += NT)
                 ct64_stage2<S, T>(sm, N, t, coladdr, [&](int p, int k, cx<T> v) {
-                    st_cg_hint(reinterpret_cast<double2 *>(dst + k * N + ct64_slot(p)), make_double2(v.re, v.im),
-                               pol_last);
+                    cx<T> *o = dst + k * N + ct64_slot(p);
+                    if constexpr (sizeof(T) == 8)
+                        st_cg_hint(reinterpret_cast<double2 *>(o), make_double2(v.re, v.im), pol_last);
+                    else
+                        st_cg_hint(reinterpret_cast<float2 *>(o), make_float2(v.re, v.im), pol_last);
                 });
             fence_proxy_async_smem();  // these reads before the next item's bulk copies
             __syncthreads();  // then one cumulative release publishes every thread's stores
@@ -1088,19 +1092,19 @@ static void add_twopass_pfa(std::vector<KernelEntry> &out, const char *name)
     add_twopass_pfa<-1, G, NT, MINB>(out, "twopass 36x36x36 double g" #G " pfa nt" #NT " minb" #MINB); \
     add_twopass_pfa<+1, G, NT, MINB>(out, "twopass 36x36x36 double g" #G " pfa nt" #NT " minb" #MINB)
 
-template <int S, int NT, int MINB>
+template <int S, int NT, int MINB, typename T = double>
 static void add_twopass_ct64(std::vector<KernelEntry> &out, const char *name)
 {
     KernelEntry e;
     e.n0 = e.n1 = e.n2 = 64;
-    e.precision = FFT3D_B200_C128;
+    e.precision = sizeof(T) == 8 ? FFT3D_B200_C128 : FFT3D_B200_C64;
     e.sign = S;
     e.family = FAM_TWOPASS;  // same launch arguments and workspace as k_twopass
     e.alg = 512;
     e.vpc = 1;
     e.threads = NT;
-    e.smem = 64 * 65 * (int)sizeof(cx<double>);
-    e.func = (const void *)&k_twopass_ct64<S, NT, MINB>;
+    e.smem = 64 * (sizeof(T) == 8 ? 65 : 66) * (int)sizeof(cx<T>);
+    e.func = (const void *)&k_twopass_ct64<S, NT, MINB, T>;
     e.name = name;
     out.push_back(e);
 }
@@ -1109,6 +1113,9 @@ static void add_twopass_ct64(std::vector<KernelEntry> &out, const char *name)
 #define FFT3D_TWOPASS_CT64(NT, MINB)                                                               \
     add_twopass_ct64<-1, NT, MINB>(out, "twopass 64x64x64 double g1 ct nt" #NT " minb" #MINB);    \
     add_twopass_ct64<+1, NT, MINB>(out, "twopass 64x64x64 double g1 ct nt" #NT " minb" #MINB)
+#define FFT3D_TWOPASS_CT64_F(NT, MINB)                                                             \
+    add_twopass_ct64<-1, NT, MINB, float>(out, "twopass 64x64x64 float g1 ct nt" #NT " minb" #MINB); \
+    add_twopass_ct64<+1, NT, MINB, float>(out, "twopass 64x64x64 float g1 ct nt" #NT " minb" #MINB)
 
 // Rows moved by bulk copies (complex double, row-major layouts): "bulk" in the name.
 #define FFT3D_TWOPASS_BULK(N0, N1, N2, G, NT, MINB)                                              \
@@ -1150,6 +1157,8 @@ void register_twopass_kernels(std::vector<KernelEntry> &out)
     FFT3D_TWOPASS_CT64(256, 3);
     FFT3D_TWOPASS_CT64(384, 2);
     FFT3D_TWOPASS_CT64(128, 3);
+    FFT3D_TWOPASS_CT64_F(128, 6);
+    FFT3D_TWOPASS_CT64_F(256, 3);
     // 36-point lines as 4 x 9 stages: ~85 registers, 24 warps per SM
     FFT3D_TWOPASS_PFA36(3, 256, 3);
     FFT3D_TWOPASS_PFA36(2, 256, 4);

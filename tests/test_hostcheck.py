@@ -192,9 +192,9 @@ def test_twopass_pfa36_stages(hostcheck, g, nvol, sign):
     assert oracle.rel_error_per_volume(got, want).max() < C128_TOL
 
 
-@pytest.mark.parametrize("nvol", [1, 3])
+@pytest.mark.parametrize("nvol,prec", [(1, 0), (3, 0), (2, 1)])
 @pytest.mark.parametrize("sign", [-1, +1])
-def test_twopass_ct64_stages(hostcheck, nvol, sign):
+def test_twopass_ct64_stages(hostcheck, nvol, prec, sign):
     """64^3 TWOPASS with every line split into its 8 x 8 Cooley-Tukey stages
     (alg = 701): the twiddles and index maps of ct64.cuh, the digit-reversed
     in-place z pass and the natural-order stores, in ticket order with the
@@ -203,11 +203,13 @@ def test_twopass_ct64_stages(hostcheck, nvol, sign):
     hostcheck.hostcheck_twopass_violations.restype = ctypes.c_longlong
     hostcheck.hostcheck_twopass_violations()
     rng = np.random.default_rng(9000 + nvol)
-    x = field(rng, (nvol, 64, 64, 64), dist="normal")
-    got = run(hostcheck, x, (64, 64, 64), 0, sign, 701, 1)
+    dt = np.complex128 if prec == 0 else np.complex64
+    x = field(rng, (nvol, 64, 64, 64), dist="normal", dtype=dt)
+    got = run(hostcheck, x, (64, 64, 64), prec, sign, 701, 1)
     assert hostcheck.hostcheck_twopass_violations() == 0
-    want = oracle.fft3d(x) if sign < 0 else oracle.ifft3d(x)
-    assert oracle.rel_error_per_volume(got, want).max() < C128_TOL
+    x64 = x.astype(np.complex128)
+    want = oracle.fft3d(x64) if sign < 0 else oracle.ifft3d(x64)
+    assert oracle.rel_error_per_volume(got, want).max() < (C128_TOL if prec == 0 else C64_TOL)
 
 
 SPLIT = [((36, 36, 36), 0, 2, 11), ((36, 36, 36), 0, 1, 3), ((36, 36, 36), 1, 4, 5),

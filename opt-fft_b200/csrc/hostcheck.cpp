@@ -11,7 +11,7 @@
 
 #include <vector>
 
-#include "ct64.cuh"
+#include "staged.cuh"
 #include "mgpu.cuh"
 #include "pfa36.cuh"
 #include "splitline.cuh"
@@ -296,15 +296,15 @@ static void emulate_twopass_pfa(const void *vin, void *vout, long long nvol)
     }
 }
 
-// The 64^3 TWOPASS variant with lines split into 8 x 8 stages
-// (k_twopass_ct64): rows at pitch 65, z pass in place (rows end in ct64_slot
-// order), y pass stored into the slot at the natural z, x pass streamed out;
-// every stage-1 task of a pass before any stage-2 task, as the kernel's
-// barrier orders them.  Tickets, ring and dependency checks as emulate_twopass.
-template <int S, typename T = double>
-static void emulate_twopass_ct64(const void *vin, void *vout, long long nvol)
+// The staged TWOPASS kernel (k_twopass_staged; staged.cuh line policies):
+// rows at the kernel's pitch, z pass in place (rows end in Line::slot order),
+// y pass stored into the slot at the natural z, x pass streamed out; every
+// stage-1 task of a pass before any stage-2 task, as the kernel's barrier
+// orders them.  Tickets, ring and dependency checks as emulate_twopass.
+template <class Line, int S, typename T = double>
+static void emulate_twopass_staged(const void *vin, void *vout, long long nvol)
 {
-    constexpr int N = 64, P = sizeof(T) == 8 ? N + 1 : N + 2;
+    constexpr int N = Line::N, P = sizeof(T) == 8 ? (N | 1) : ((N + 2) & ~1);
     constexpr long long PLANE = (long long)N * N;
     using TG = TwoPassGeom<N, N, N, T, 1>;
     const T scale = S > 0 ? T(1) / T(TG::V) : T(1);
@@ -331,20 +331,20 @@ static void emulate_twopass_ct64(const void *vin, void *vout, long long nvol)
             const cx<T> *rows = in + it.vol * TG::V + (long long)it.j * PLANE;
             for (int r = 0; r < N; ++r)
                 for (int z = 0; z < N; ++z) sm[r * P + z] = rows[(long long)r * N + z];
-            for (int q = 0; q < N * 8; ++q) ct64_stage1<S, T>(sm, N, q, rowaddr);
-            for (int q = 0; q < N * 8; ++q)
-                ct64_stage2<S, T>(sm, N, q, rowaddr, [&](int l, int k, cx<T> v) { sm[rowaddr(l, ct64_slot(k))] = v; });
-            for (int q = 0; q < N * 8; ++q) ct64_stage1<S, T>(sm, N, q, coladdr);
+            for (int q = 0; q < N * Line::T1; ++q) Line::template stage1<S, T>(sm, N, q, rowaddr);
+            for (int q = 0; q < N * Line::T2; ++q)
+                Line::template stage2<S, T>(sm, N, q, rowaddr, [&](int l, int k, cx<T> v) { sm[rowaddr(l, Line::slot(k))] = v; });
+            for (int q = 0; q < N * Line::T1; ++q) Line::template stage1<S, T>(sm, N, q, coladdr);
             cx<T> *dst = sv + (long long)it.j * PLANE;
-            for (int q = 0; q < N * 8; ++q)
-                ct64_stage2<S, T>(sm, N, q, coladdr, [&](int p, int k, cx<T> v) { dst[k * N + ct64_slot(p)] = v; });
+            for (int q = 0; q < N * Line::T2; ++q)
+                Line::template stage2<S, T>(sm, N, q, coladdr, [&](int p, int k, cx<T> v) { dst[k * N + Line::at(p)] = v; });
         } else {
             for (int x = 0; x < N; ++x)
                 for (int z = 0; z < N; ++z) sm[x * P + z] = sv[((long long)x * N + it.j) * N + z];
-            for (int q = 0; q < N * 8; ++q) ct64_stage1<S, T>(sm, N, q, coladdr);
+            for (int q = 0; q < N * Line::T1; ++q) Line::template stage1<S, T>(sm, N, q, coladdr);
             cx<T> *gvol = out + it.vol * TG::V + (long long)it.j * N;
-            for (int q = 0; q < N * 8; ++q)
-                ct64_stage2<S, T>(sm, N, q, coladdr, [&](int z, int k, cx<T> v) {
+            for (int q = 0; q < N * Line::T2; ++q)
+                Line::template stage2<S, T>(sm, N, q, coladdr, [&](int z, int k, cx<T> v) {
                     if (S > 0) v = cscale(v, scale);
                     gvol[k * PLANE + z] = v;
                 });
@@ -446,10 +446,9 @@ typedef void (*emu_fn)(const void *, void *, long long);
 #define EMU_TPP(G)                                                                            \
     {36, 36, 36, 0, -1, 600 + G, 1, &emulate_twopass_pfa<-1, G>},                               \
     {36, 36, 36, 0, +1, 600 + G, 1, &emulate_twopass_pfa<+1, G>}
-#define EMU_TPCT64                                                                            \
-    {64, 64, 64, 0, -1, 701, 1, &emulate_twopass_ct64<-1>}, {64, 64, 64, 0, +1, 701, 1, &emulate_twopass_ct64<+1>}, \
-    {64, 64, 64, 1, -1, 701, 1, &emulate_twopass_ct64<-1, float>},                                \
-    {64, 64, 64, 1, +1, 701, 1, &emulate_twopass_ct64<+1, float>}
+#define EMU_TPST(LINE, N, T)                                                                  \
+    {N, N, N, sizeof(T) == 8 ? 0 : 1, -1, 701, 1, &emulate_twopass_staged<LINE, -1, T>},         \
+    {N, N, N, sizeof(T) == 8 ? 0 : 1, +1, 701, 1, &emulate_twopass_staged<LINE, +1, T>}
 #define EMU_TP(N0, N1, N2, T, G)                                                              \
     {N0, N1, N2, sizeof(T) == 8 ? 0 : 1, -1, 300 + G, 1,                                    \
      &emulate_twopass<N0, N1, N2, T, -1, G>},                                                \
@@ -497,7 +496,7 @@ static const EmuEntry kEmu[] = {
     EMU_TPS(36, 36, 36, double, 2), EMU_TPS(36, 36, 36, double, 1), EMU_TPS(36, 36, 36, float, 4),
     EMU_TPS(64, 64, 64, double, 1), EMU_TPS(64, 64, 64, float, 2),  EMU_TPS(36, 36, 64, double, 2),
     EMU_TPR(36, 36, 36, 3), EMU_TPR(36, 36, 36, 2), EMU_TPR(36, 36, 36, 4), EMU_TPRP(36, 36, 36, 3), EMU_TPRP(36, 36, 36, 2), EMU_TPRQ(36, 36, 36, 3),
-    EMU_TPRQ(36, 36, 36, 2), EMU_TPRP(45, 45, 45, 3), EMU_TPRP(6, 9, 5, 3), EMU_TPRQ(6, 9, 5, 3), EMU_TPRQF(3), EMU_TPRQF(2), EMU_TPRQF(4), EMU_TPP(2), EMU_TPP(3), EMU_TPP(4), EMU_TPCT64,
+    EMU_TPRQ(36, 36, 36, 2), EMU_TPRP(45, 45, 45, 3), EMU_TPRP(6, 9, 5, 3), EMU_TPRQ(6, 9, 5, 3), EMU_TPRQF(3), EMU_TPRQF(2), EMU_TPRQF(4), EMU_TPP(2), EMU_TPP(3), EMU_TPP(4), EMU_TPST(LineCT64, 64, double), EMU_TPST(LineCT64, 64, float), EMU_TPST(LinePFA45, 45, double),
     EMU_TPR(6, 9, 5, 3),
 };
 

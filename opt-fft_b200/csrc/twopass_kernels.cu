@@ -22,11 +22,11 @@
 // launch, on the error path as well.
 #include <algorithm>
 
-#include "ct64.cuh"
 #include "internal.h"
 #include "pfa36.cuh"
 #include "ptx.cuh"
 #include "splitline.cuh"
+#include "staged.cuh"
 #include "twopass.cuh"
 
 namespace fft3d {
@@ -788,24 +788,29 @@ __global__ void __launch_bounds__(NT, MINB)
     }
 }
 
-// TWOPASS for 64^3 complex double with every 64-point line split into its
-// 8 x 8 Cooley-Tukey stages (ct64.cuh): one plane or one y-row per item, eight
-// points per thread task, ~85 registers, 24 warps per SM -- where a 64-point
-// line in one thread spills about 1.3 KB.  Rows are held at an odd pitch of 65
-// points (bank-conflict-free for rows and columns) and moved by bulk copies.
-// The z pass runs in place, leaving each row in ct64_slot order; the y pass's
-// second stage stores into the scratch slot at the natural z; the row item's
-// second stage streams the output.  Item control, L2 policies and the slot
-// release as in k_twopass_regs.
-template <int S, int NT, int MINB, typename T = double>
+// TWOPASS for N^3 with every line split into two thread-level stages
+// (staged.cuh: 64 = 8 x 8 Cooley-Tukey, 45 = 5 x 9 Good-Thomas): one plane or
+// one y-row per item, a task holds 5 to 9 points, so many warps fit an SM --
+// where an N-point line in one thread spills (64) or leaves 8 warps per SM
+// (45).  Rows are held at pitch P (odd for complex double: bank-conflict-free
+// rows and columns; even for complex float, whose rows must start 16-byte
+// aligned for the bulk copies) and moved by bulk copies.  The z pass runs in
+// place, leaving each row in Line::slot order; the y pass's second stage
+// stores into the scratch slot at the natural z; the row item's second stage
+// streams the output.  Item control, L2 policies and the slot release as in
+// k_twopass_regs.
+template <class Line, typename T>
+constexpr int staged_pitch() { return sizeof(T) == 8 ? (Line::N | 1) : ((Line::N + 2) & ~1); }
+
+template <class Line, int S, int NT, int MINB, typename T = double>
 __global__ void __launch_bounds__(NT, MINB)
-    k_twopass_ct64(const cx<T> *__restrict__ in, cx<T> *__restrict__ out, long long nvol, T scale,
-                   int *err, unsigned char *work, int R, int D)
+    k_twopass_staged(const cx<T> *__restrict__ in, cx<T> *__restrict__ out, long long nvol, T scale,
+                     int *err, unsigned char *work, int R, int D)
 {
     pdl_begin();
-    // row pitch: odd for 16-byte points; 66 for 8-byte points, whose rows must
-    // still start 16-byte aligned for the bulk copies
-    constexpr int N = 64, P = sizeof(T) == 8 ? N + 1 : N + 2;
+    constexpr int N = Line::N, P = staged_pitch<Line, T>();
+    static_assert((N * sizeof(cx<T>)) % 16 == 0 && (P * sizeof(cx<T>)) % 16 == 0,
+                  "bulk row copies: 16-byte rows at 16-byte aligned shared-memory starts");
     using TG = TwoPassGeom<N, N, N, T, 1>;
     static_assert(NT % 32 == 0, "whole warps");
     constexpr uint32_t ROW_BYTES = (uint32_t)(N * sizeof(cx<T>));
@@ -874,19 +879,20 @@ __global__ void __launch_bounds__(NT, MINB)
             if (!wait_copies()) s_stop = 2;
             __syncthreads();
             if (s_stop) break;
-            // 2. z pass along the rows, in place (rows end in ct64_slot order)
-            for (int t = tid; t < N * 8; t += NT) ct64_stage1<S, T>(sm, N, t, rowaddr);
+            // 2. z pass along the rows, in place (rows end in Line::slot order)
+            for (int t = tid; t < N * Line::T1; t += NT) Line::template stage1<S, T>(sm, N, t, rowaddr);
             __syncthreads();
-            for (int t = tid; t < N * 8; t += NT)
-                ct64_stage2<S, T>(sm, N, t, rowaddr, [&](int l, int k, cx<T> v) { sm[rowaddr(l, ct64_slot(k))] = v; });
+            for (int t = tid; t < N * Line::T2; t += NT)
+                Line::template stage2<S, T>(sm, N, t, rowaddr,
+                                            [&](int l, int k, cx<T> v) { sm[rowaddr(l, Line::slot(k))] = v; });
             __syncthreads();
-            // 3. y pass along the columns; column p holds z = ct64_slot(p)
-            for (int t = tid; t < N * 8; t += NT) ct64_stage1<S, T>(sm, N, t, coladdr);
+            // 3. y pass along the columns; column p holds z = Line::at(p)
+            for (int t = tid; t < N * Line::T1; t += NT) Line::template stage1<S, T>(sm, N, t, coladdr);
             __syncthreads();
             cx<T> *dst = sv + (long long)it.j * PLANE;
-            for (int t = tid; t < N * 8; t += NT)
-                ct64_stage2<S, T>(sm, N, t, coladdr, [&](int p, int k, cx<T> v) {
-                    cx<T> *o = dst + k * N + ct64_slot(p);
+            for (int t = tid; t < N * Line::T2; t += NT)
+                Line::template stage2<S, T>(sm, N, t, coladdr, [&](int p, int k, cx<T> v) {
+                    cx<T> *o = dst + k * N + Line::at(p);
                     if constexpr (sizeof(T) == 8)
                         st_cg_hint(reinterpret_cast<double2 *>(o), make_double2(v.re, v.im), pol_last);
                     else
@@ -908,11 +914,11 @@ __global__ void __launch_bounds__(NT, MINB)
             // the slot may be overwritten: its rows are in shared memory
             if (tid == 0) red_release_gpu_add(&ctl->cnt[TWOPASS_RMAX + slot], 1u);
             // 2. x pass along the columns (column z), streamed to the output
-            for (int t = tid; t < N * 8; t += NT) ct64_stage1<S, T>(sm, N, t, coladdr);
+            for (int t = tid; t < N * Line::T1; t += NT) Line::template stage1<S, T>(sm, N, t, coladdr);
             __syncthreads();
             cx<T> *gvol = out + it.vol * TG::V + (long long)it.j * N;
-            for (int t = tid; t < N * 8; t += NT)
-                ct64_stage2<S, T>(sm, N, t, coladdr, [&](int z, int k, cx<T> v) {
+            for (int t = tid; t < N * Line::T2; t += NT)
+                Line::template stage2<S, T>(sm, N, t, coladdr, [&](int z, int k, cx<T> v) {
                     if constexpr (S > 0) v = cscale(v, scale);
                     store_out(gvol + k * PLANE + z, v);
                 });
@@ -1092,30 +1098,29 @@ static void add_twopass_pfa(std::vector<KernelEntry> &out, const char *name)
     add_twopass_pfa<-1, G, NT, MINB>(out, "twopass 36x36x36 double g" #G " pfa nt" #NT " minb" #MINB); \
     add_twopass_pfa<+1, G, NT, MINB>(out, "twopass 36x36x36 double g" #G " pfa nt" #NT " minb" #MINB)
 
-template <int S, int NT, int MINB, typename T = double>
-static void add_twopass_ct64(std::vector<KernelEntry> &out, const char *name)
+template <class Line, int S, int NT, int MINB, typename T = double>
+static void add_twopass_staged(std::vector<KernelEntry> &out, const char *name)
 {
     KernelEntry e;
-    e.n0 = e.n1 = e.n2 = 64;
+    e.n0 = e.n1 = e.n2 = Line::N;
     e.precision = sizeof(T) == 8 ? FFT3D_B200_C128 : FFT3D_B200_C64;
     e.sign = S;
     e.family = FAM_TWOPASS;  // same launch arguments and workspace as k_twopass
     e.alg = 512;
     e.vpc = 1;
     e.threads = NT;
-    e.smem = 64 * (sizeof(T) == 8 ? 65 : 66) * (int)sizeof(cx<T>);
-    e.func = (const void *)&k_twopass_ct64<S, NT, MINB, T>;
+    e.smem = Line::N * staged_pitch<Line, T>() * (int)sizeof(cx<T>);
+    e.func = (const void *)&k_twopass_staged<Line, S, NT, MINB, T>;
     e.name = name;
     out.push_back(e);
 }
 
-// 64^3 complex double, lines split into their 8 x 8 stages: "ct" in the name.
-#define FFT3D_TWOPASS_CT64(NT, MINB)                                                               \
-    add_twopass_ct64<-1, NT, MINB>(out, "twopass 64x64x64 double g1 ct nt" #NT " minb" #MINB);    \
-    add_twopass_ct64<+1, NT, MINB>(out, "twopass 64x64x64 double g1 ct nt" #NT " minb" #MINB)
-#define FFT3D_TWOPASS_CT64_F(NT, MINB)                                                             \
-    add_twopass_ct64<-1, NT, MINB, float>(out, "twopass 64x64x64 float g1 ct nt" #NT " minb" #MINB); \
-    add_twopass_ct64<+1, NT, MINB, float>(out, "twopass 64x64x64 float g1 ct nt" #NT " minb" #MINB)
+// Lines split into two stages: "ct" (64 = 8 x 8) or "pfa" (45 = 5 x 9) in the name.
+#define FFT3D_TWOPASS_STAGED(LINE, N, T, KIND, NT, MINB)                                           \
+    add_twopass_staged<LINE, -1, NT, MINB, T>(out, "twopass " #N "x" #N "x" #N " " #T " g1 " KIND  \
+                                                   " nt" #NT " minb" #MINB);                        \
+    add_twopass_staged<LINE, +1, NT, MINB, T>(out, "twopass " #N "x" #N "x" #N " " #T " g1 " KIND  \
+                                                   " nt" #NT " minb" #MINB)
 
 // Rows moved by bulk copies (complex double, row-major layouts): "bulk" in the name.
 #define FFT3D_TWOPASS_BULK(N0, N1, N2, G, NT, MINB)                                              \
@@ -1153,12 +1158,15 @@ void register_twopass_kernels(std::vector<KernelEntry> &out)
     FFT3D_TWOPASS_BULKQ(36, 36, 36, 3, 128, 3);
     FFT3D_TWOPASS_BULKQ(36, 36, 36, 2, 96, 4);
     FFT3D_TWOPASS_BULKP(45, 45, 45, 3, 160, 2);
-    // 64-point lines as 8 x 8 stages: one plane or y-row per item, 24 warps per SM
-    FFT3D_TWOPASS_CT64(256, 3);
-    FFT3D_TWOPASS_CT64(384, 2);
-    FFT3D_TWOPASS_CT64(128, 3);
-    FFT3D_TWOPASS_CT64_F(128, 6);
-    FFT3D_TWOPASS_CT64_F(256, 3);
+    // 64-point lines as 8 x 8 stages: one plane or y-row per item
+    FFT3D_TWOPASS_STAGED(LineCT64, 64, double, "ct", 256, 3);
+    FFT3D_TWOPASS_STAGED(LineCT64, 64, double, "ct", 384, 2);
+    FFT3D_TWOPASS_STAGED(LineCT64, 64, double, "ct", 128, 3);
+    FFT3D_TWOPASS_STAGED(LineCT64, 64, float, "ct", 128, 6);
+    FFT3D_TWOPASS_STAGED(LineCT64, 64, float, "ct", 256, 3);
+    // 45-point lines as 5 x 9 stages: one plane or y-row per item (complex
+    // double only: a 45-point complex-float row, 360 bytes, cannot be a bulk copy)
+    FFT3D_TWOPASS_STAGED(LinePFA45, 45, double, "pfa", 128, 6);
     // 36-point lines as 4 x 9 stages: ~85 registers, 24 warps per SM
     FFT3D_TWOPASS_PFA36(3, 256, 3);
     FFT3D_TWOPASS_PFA36(2, 256, 4);

@@ -192,20 +192,24 @@ def test_twopass_pfa36_stages(hostcheck, g, nvol, sign):
     assert oracle.rel_error_per_volume(got, want).max() < C128_TOL
 
 
-@pytest.mark.parametrize("nvol,prec", [(1, 0), (3, 0), (2, 1)])
+STAGED = [(64, 1, 0), (64, 3, 0), (64, 2, 1), (45, 3, 0), (45, 1, 0)]
+
+
+@pytest.mark.parametrize("n,nvol,prec", STAGED, ids=[f"{t[0]}-b{t[1]}-p{t[2]}" for t in STAGED])
 @pytest.mark.parametrize("sign", [-1, +1])
-def test_twopass_ct64_stages(hostcheck, nvol, prec, sign):
-    """64^3 TWOPASS with every line split into its 8 x 8 Cooley-Tukey stages
-    (alg = 701): the twiddles and index maps of ct64.cuh, the digit-reversed
-    in-place z pass and the natural-order stores, in ticket order with the
-    dependency check."""
+def test_twopass_staged_lines(hostcheck, n, nvol, prec, sign):
+    """TWOPASS with every line split into two thread-level stages (alg = 701):
+    64 = 8 x 8 Cooley-Tukey and 45 = 5 x 9 Good-Thomas (staged.cuh) -- the
+    twiddles and index maps, the permuted in-place z pass and the natural-order
+    stores, both precisions' row pitches, in ticket order with the dependency
+    check."""
     import ctypes
     hostcheck.hostcheck_twopass_violations.restype = ctypes.c_longlong
     hostcheck.hostcheck_twopass_violations()
-    rng = np.random.default_rng(9000 + nvol)
+    rng = np.random.default_rng(9000 + n + nvol)
     dt = np.complex128 if prec == 0 else np.complex64
-    x = field(rng, (nvol, 64, 64, 64), dist="normal", dtype=dt)
-    got = run(hostcheck, x, (64, 64, 64), prec, sign, 701, 1)
+    x = field(rng, (nvol, n, n, n), dist="normal", dtype=dt)
+    got = run(hostcheck, x, (n, n, n), prec, sign, 701, 1)
     assert hostcheck.hostcheck_twopass_violations() == 0
     x64 = x.astype(np.complex128)
     want = oracle.fft3d(x64) if sign < 0 else oracle.ifft3d(x64)

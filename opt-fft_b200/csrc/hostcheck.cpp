@@ -13,7 +13,6 @@
 
 #include "staged.cuh"
 #include "mgpu.cuh"
-#include "pfa36.cuh"
 #include "splitline.cuh"
 #include "twopass.cuh"
 #include "volume.cuh"
@@ -232,70 +231,6 @@ static void emulate_twopass_regs(const void *vin, void *vout, long long nvol)
     }
 }
 
-// The 36^3 TWOPASS variant with lines split into 4 x 9 stages
-// (k_twopass_pfa): every stage-1 task of a pass, then every stage-2 task, as
-// the kernel's barrier between them orders them; tickets, ring and dependency
-// checks as emulate_twopass.
-template <int S, int G>
-static void emulate_twopass_pfa(const void *vin, void *vout, long long nvol)
-{
-    constexpr int N = 36, LINES = G * N;
-    constexpr long long PLANE = (long long)N * N;
-    using T = double;
-    using TG = TwoPassGeom<N, N, N, T, G>;
-    using XG = typename TG::XG;
-    using YG = typename TG::YG;
-    const T scale = S > 0 ? T(1) / T(TG::V) : T(1);
-    int lag = 0;
-    const int R = twopass_ring_size(TG::NA, TG::NB, 7, &lag);
-    std::vector<cx<T>> smv((size_t)TG::PV), ring((size_t)R * TG::V, cx<T>{T(-777.0), T(555.0)});
-    cx<T> *sm = smv.data();
-    const cx<T> *in = (const cx<T> *)vin;
-    cx<T> *out = (cx<T> *)vout;
-    const long long total = (long long)(TG::NA + TG::NB) * nvol;
-    std::vector<long long> cnt_plane(R, 0), cnt_row(R, 0);
-    auto zaddr = [](int l, int e) { return XG::off(l, e); };
-    auto yaddr = [](int l, int e) { return XG::off((l / N) * N + e, l % N); };
-    auto xaddr = [](int l, int e) { return YG::off(e * G + l / N, l % N); };
-    for (long long t = 0; t < total; ++t) {
-        const TwoPassItem it = twopass_decode(t, nvol, TG::NA, TG::NB, lag);
-        const int slot = (int)(it.vol % R);
-        const long long round = it.vol / R;
-        cx<T> *sv = ring.data() + slot * TG::V;
-        if (it.plane ? cnt_row[slot] < TG::NB * round : cnt_plane[slot] < TG::NA * (round + 1))
-            g_twopass_violations++;
-        (it.plane ? cnt_plane : cnt_row)[slot]++;
-        for (auto &e : smv) e = {T(12345.0), T(-6789.0)};
-        if (it.plane) {
-            const cx<T> *rows = in + it.vol * TG::V + (long long)it.j * G * PLANE;
-            for (int r = 0; r < G * N; ++r)
-                for (int z = 0; z < N; ++z) sm[XG::off(r, z)] = rows[(long long)r * N + z];
-            for (int q = 0; q < LINES * 9; ++q) pfa36_stage1<S, T>(sm, LINES, q, zaddr);
-            for (int q = 0; q < LINES * 4; ++q)
-                pfa36_stage2<S, T>(sm, LINES, q, zaddr, [&](int l, int k, cx<T> v) { sm[zaddr(l, k)] = v; });
-            for (int q = 0; q < LINES * 9; ++q) pfa36_stage1<S, T>(sm, LINES, q, yaddr);
-            cx<T> *dst = sv + (long long)it.j * G * PLANE;
-            for (int q = 0; q < LINES * 4; ++q)
-                pfa36_stage2<S, T>(sm, LINES, q, yaddr, [&](int l, int k, cx<T> v) {
-                    store_l2(dst + (long long)(l / N) * PLANE + k * N + l % N, v);
-                });
-        } else {
-            for (int q = 0; q < G * N; ++q) {
-                const int x = q / G, yl = q % G;
-                for (int z = 0; z < N; ++z)
-                    sm[YG::off(q, z)] = sv[((long long)x * N + it.j * G + yl) * N + z];
-            }
-            for (int q = 0; q < LINES * 9; ++q) pfa36_stage1<S, T>(sm, LINES, q, xaddr);
-            cx<T> *gvol = out + it.vol * TG::V + (long long)it.j * G * N;
-            for (int q = 0; q < LINES * 4; ++q)
-                pfa36_stage2<S, T>(sm, LINES, q, xaddr, [&](int l, int k, cx<T> v) {
-                    if (S > 0) v = cscale(v, scale);
-                    gvol[k * PLANE + l] = v;
-                });
-        }
-    }
-}
-
 // The staged TWOPASS kernel (k_twopass_staged; staged.cuh line policies):
 // rows at the kernel's pitch, z pass in place (rows end in Line::slot order),
 // y pass stored into the slot at the natural z, x pass streamed out; every
@@ -443,9 +378,6 @@ typedef void (*emu_fn)(const void *, void *, long long);
 #define EMU_TPRQF(G)                                                                          \
     {36, 36, 36, 1, -1, 540 + G, 1, &emulate_twopass_regs<36, 36, 36, float, -1, G, true, true, 38>},  \
     {36, 36, 36, 1, +1, 540 + G, 1, &emulate_twopass_regs<36, 36, 36, float, +1, G, true, true, 38>}
-#define EMU_TPP(G)                                                                            \
-    {36, 36, 36, 0, -1, 600 + G, 1, &emulate_twopass_pfa<-1, G>},                               \
-    {36, 36, 36, 0, +1, 600 + G, 1, &emulate_twopass_pfa<+1, G>}
 #define EMU_TPST(LINE, N, T)                                                                  \
     {N, N, N, sizeof(T) == 8 ? 0 : 1, -1, 701, 1, &emulate_twopass_staged<LINE, -1, T>},         \
     {N, N, N, sizeof(T) == 8 ? 0 : 1, +1, 701, 1, &emulate_twopass_staged<LINE, +1, T>}
@@ -496,7 +428,8 @@ static const EmuEntry kEmu[] = {
     EMU_TPS(36, 36, 36, double, 2), EMU_TPS(36, 36, 36, double, 1), EMU_TPS(36, 36, 36, float, 4),
     EMU_TPS(64, 64, 64, double, 1), EMU_TPS(64, 64, 64, float, 2),  EMU_TPS(36, 36, 64, double, 2),
     EMU_TPR(36, 36, 36, 3), EMU_TPR(36, 36, 36, 2), EMU_TPR(36, 36, 36, 4), EMU_TPRP(36, 36, 36, 3), EMU_TPRP(36, 36, 36, 2), EMU_TPRQ(36, 36, 36, 3),
-    EMU_TPRQ(36, 36, 36, 2), EMU_TPRP(45, 45, 45, 3), EMU_TPRP(6, 9, 5, 3), EMU_TPRQ(6, 9, 5, 3), EMU_TPRQF(3), EMU_TPRQF(2), EMU_TPRQF(4), EMU_TPP(2), EMU_TPP(3), EMU_TPP(4), EMU_TPST(LineCT64, 64, double), EMU_TPST(LineCT64, 64, float), EMU_TPST(LinePFA45, 45, double),
+    EMU_TPRQ(36, 36, 36, 2), EMU_TPRP(45, 45, 45, 3), EMU_TPRP(6, 9, 5, 3), EMU_TPRQ(6, 9, 5, 3), EMU_TPRQF(3), EMU_TPRQF(2), EMU_TPRQF(4), EMU_TPST(LineCT64, 64, double), EMU_TPST(LineCT64, 64, float), EMU_TPST(LinePFA45, 45, double),
+    EMU_TPST(LinePFA36, 36, double), EMU_TPST(LinePFA36, 36, float),
     EMU_TPR(6, 9, 5, 3),
 };
 

@@ -23,7 +23,6 @@
 #include <algorithm>
 
 #include "internal.h"
-#include "pfa36.cuh"
 #include "ptx.cuh"
 #include "splitline.cuh"
 #include "staged.cuh"
@@ -640,154 +639,6 @@ __global__ void __launch_bounds__(NT, MINB)
     }
 }
 
-// TWOPASS for 36^3 complex double with every 36-point line split into its
-// 4 x 9 prime-factor stages (pfa36.cuh): a thread task holds 4 or 9 points, so
-// the kernel runs in ~85 registers and three 256-thread CTAs (24 warps) share
-// an SM, where one-thread-per-line kernels keep 12 warps.  Items, tickets
-// (taken one ahead), waits and bulk row copies as in k_twopass_regs; the y
-// pass's second stage stores into the scratch slot (L2 only), and the row
-// item's rows come back by bulk copies, its second stage streaming the output.
-template <int S, int G, int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB)
-    k_twopass_pfa(const cx<double> *__restrict__ in, cx<double> *__restrict__ out, long long nvol,
-                  double scale, int *err, unsigned char *work, int R, int D)
-{
-    pdl_begin();
-    constexpr int N = 36;
-    using T = double;
-    using TG = TwoPassGeom<N, N, N, T, G>;
-    using XG = typename TG::XG;
-    using YG = typename TG::YG;
-    static_assert(XG::POL == 1 && YG::POL == 1 && NT % 32 == 0, "row pitch 37, whole warps");
-    constexpr uint32_t ROW_BYTES = (uint32_t)(N * sizeof(cx<T>));
-    constexpr int LINES = G * N;  // lines per pass of an item
-    constexpr long long PLANE = (long long)N * N;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);
-    __shared__ long long s_t;
-    __shared__ int s_stop;
-    __shared__ __align__(8) uint64_t s_bar;
-    TwoPassCtl *ctl = reinterpret_cast<TwoPassCtl *>(work);
-    cx<T> *ring = reinterpret_cast<cx<T> *>(work + TWOPASS_CTL_BYTES);
-    const int tid = threadIdx.x;
-    const long long total = (long long)(TG::NA + TG::NB) * nvol;
-    uint32_t phase = 0;
-    bool copies_pending = false;
-    long long next = 0;  // thread 0: the ticket taken ahead
-    if (tid == 0) {
-        mbar_init(&s_bar, 1);
-        fence_mbar_init();
-        next = (long long)atomicAdd(&ctl->ticket, 1ull);
-    }
-    // element e of line l in each pass's layout
-    auto zaddr = [](int l, int e) { return XG::off(l, e); };              // l = row (g, y)
-    auto yaddr = [](int l, int e) { return XG::off((l / N) * N + e, l % N); };  // l = (g, z)
-    auto xaddr = [](int l, int e) { return YG::off(e * G + l / N, l % N); };    // l = (yl, z)
-
-    for (;;) {
-        if (tid == 0) {
-            const long long t = next;
-            int stop = (t >= total || ld_acquire_gpu(&ctl->abort) != 0) ? 1 : 0;
-            if (!stop) {
-                next = (long long)atomicAdd(&ctl->ticket, 1ull);
-                const TwoPassItem it = twopass_decode(t, nvol, TG::NA, TG::NB, D);
-                const int slot = (int)(it.vol % R);
-                const unsigned round = (unsigned)(it.vol / R);
-                const bool ok =
-                    it.plane
-                        ? wait_counter_geq(&ctl->cnt[TWOPASS_RMAX + slot], (unsigned)TG::NB * round,
-                                           &ctl->abort)
-                        : wait_counter_geq(&ctl->cnt[slot], (unsigned)TG::NA * (round + 1u), &ctl->abort);
-                if (!ok) stop = 2;
-            }
-            s_t = t;
-            s_stop = stop;
-        }
-        __syncthreads();
-        if (s_stop) break;
-        const TwoPassItem it = twopass_decode(s_t, nvol, TG::NA, TG::NB, D);
-        const int slot = (int)(it.vol % R);
-        cx<T> *sv = ring + (long long)slot * TG::V;
-
-        // 1. the item's rows, one bulk copy each: G planes of the input, or
-        //    G y-rows of every plane of the scratch slot
-        if (tid == 0) mbar_arrive_expect_tx(&s_bar, (uint32_t)(G * N) * ROW_BYTES);
-        if (it.plane) {
-            const cx<T> *rows = in + it.vol * TG::V + (long long)it.j * G * PLANE;
-            for (int r = tid; r < G * N; r += NT)
-                bulk_g2s(sm + XG::off(r, 0), rows + (long long)r * N, ROW_BYTES, &s_bar);
-        } else {
-            for (int q = tid; q < G * N; q += NT) {
-                const int x = q / G, yl = q % G;
-                fence_proxy_async_global();  // the acquire above precedes these reads
-                bulk_g2s(sm + YG::off(q, 0), sv + ((long long)x * N + it.j * G + yl) * N, ROW_BYTES,
-                         &s_bar);
-            }
-        }
-        copies_pending = true;
-        const bool ok = mbar_wait_bounded(&s_bar, phase);
-        phase ^= 1u;
-        if (!ok) s_stop = 2;
-        else copies_pending = false;
-        __syncthreads();
-        if (s_stop) break;
-
-        if (it.plane) {
-            // 2. z pass, both stages in place
-            for (int t = tid; t < LINES * 9; t += NT) pfa36_stage1<S, T>(sm, LINES, t, zaddr);
-            __syncthreads();
-            for (int t = tid; t < LINES * 4; t += NT)
-                pfa36_stage2<S, T>(sm, LINES, t, zaddr, [&](int l, int k, cx<T> v) { sm[zaddr(l, k)] = v; });
-            __syncthreads();
-            // 3. y pass; its second stage stores into the scratch slot
-            for (int t = tid; t < LINES * 9; t += NT) pfa36_stage1<S, T>(sm, LINES, t, yaddr);
-            __syncthreads();
-            cx<T> *dst = sv + (long long)it.j * G * PLANE;
-            for (int t = tid; t < LINES * 4; t += NT)
-                pfa36_stage2<S, T>(sm, LINES, t, yaddr, [&](int l, int k, cx<T> v) {
-                    store_l2(dst + (long long)(l / N) * PLANE + k * N + l % N, v);
-                });
-            fence_proxy_async_smem();  // these reads before the next item's bulk copies
-            __syncthreads();  // then one cumulative release publishes every thread's stores
-            if (tid == 0) red_release_gpu_add(&ctl->cnt[slot], 1u);
-        } else {
-            // the slot's rows are in shared memory: it may be overwritten
-            if (tid == 0) red_release_gpu_add(&ctl->cnt[TWOPASS_RMAX + slot], 1u);
-            // 2. x pass; its second stage streams the output
-            for (int t = tid; t < LINES * 9; t += NT) pfa36_stage1<S, T>(sm, LINES, t, xaddr);
-            __syncthreads();
-            cx<T> *gvol = out + it.vol * TG::V + (long long)it.j * G * N;
-            for (int t = tid; t < LINES * 4; t += NT)
-                pfa36_stage2<S, T>(sm, LINES, t, xaddr, [&](int l, int k, cx<T> v) {
-                    if constexpr (S > 0) v = cscale(v, scale);
-                    store_out(gvol + k * PLANE + l, v);
-                });
-            fence_proxy_async_smem();
-            __syncthreads();
-        }
-    }
-    // a bulk copy that timed out may still land: wait once more (bounded)
-    if (copies_pending) mbar_wait_bounded(&s_bar, phase ^ 1u);
-
-    if (tid == 0 && s_stop == 2) {
-        report_error(err, DEV_ERR_DEP_TIMEOUT);
-        atomicExch(&ctl->abort, 1u);
-    }
-    // The last CTA to leave clears the control block for the next launch.
-    if (tid == 0) {
-        __threadfence();
-        const unsigned prev = atomicAdd(&ctl->done, 1u);
-        if (prev == gridDim.x - 1) {
-            __threadfence();
-            ctl->ticket = 0ull;
-            for (int i = 0; i < 2 * TWOPASS_RMAX; ++i) ctl->cnt[i] = 0u;
-            ctl->abort = 0u;
-            __threadfence();
-            ctl->done = 0u;
-        }
-    }
-}
-
 // TWOPASS for N^3 with every line split into two thread-level stages
 // (staged.cuh: 64 = 8 x 8 Cooley-Tukey, 45 = 5 x 9 Good-Thomas): one plane or
 // one y-row per item, a task holds 5 to 9 points, so many warps fit an SM --
@@ -951,7 +802,7 @@ __global__ void __launch_bounds__(NT, MINB)
 int twopass_ring(const KernelEntry &e, long long grid, int *lag)
 {
     // The lag covers up to twice the tickets the grid holds at once: kernels
-    // that take their next ticket ahead (k_twopass_regs, k_twopass_pfa) hold
+    // that take their next ticket ahead (k_twopass_regs, k_twopass_staged) hold
     // two per CTA, and for the others too a lag of two grids' worth measured
     // faster on B200 (fewer row items arriving before their planes are done).
     // It is shortened, down to one grid's worth, while the ring would exceed
@@ -1076,28 +927,6 @@ static void add_twopass_regs(std::vector<KernelEntry> &out, const char *name)
     add_twopass_regs<N0, N1, N2, +1, G, NT, MINB, true, true>(                                   \
         out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G " bulkq nt" #NT " minb" #MINB)
 
-template <int S, int G, int NT, int MINB>
-static void add_twopass_pfa(std::vector<KernelEntry> &out, const char *name)
-{
-    KernelEntry e;
-    e.n0 = e.n1 = e.n2 = 36;
-    e.precision = FFT3D_B200_C128;
-    e.sign = S;
-    e.family = FAM_TWOPASS;  // same launch arguments and workspace as k_twopass
-    e.alg = 16;
-    e.vpc = G;
-    e.threads = NT;
-    e.smem = TwoPassGeom<36, 36, 36, double, G>::SMEM;
-    e.func = (const void *)&k_twopass_pfa<S, G, NT, MINB>;
-    e.name = name;
-    out.push_back(e);
-}
-
-// 36^3 complex double, lines split into their 4 x 9 stages: "pfa" in the name.
-#define FFT3D_TWOPASS_PFA36(G, NT, MINB)                                                           \
-    add_twopass_pfa<-1, G, NT, MINB>(out, "twopass 36x36x36 double g" #G " pfa nt" #NT " minb" #MINB); \
-    add_twopass_pfa<+1, G, NT, MINB>(out, "twopass 36x36x36 double g" #G " pfa nt" #NT " minb" #MINB)
-
 template <class Line, int S, int NT, int MINB, typename T = double>
 static void add_twopass_staged(std::vector<KernelEntry> &out, const char *name)
 {
@@ -1167,12 +996,9 @@ void register_twopass_kernels(std::vector<KernelEntry> &out)
     // 45-point lines as 5 x 9 stages: one plane or y-row per item (complex
     // double only: a 45-point complex-float row, 360 bytes, cannot be a bulk copy)
     FFT3D_TWOPASS_STAGED(LinePFA45, 45, double, "pfa", 128, 6);
-    // 36-point lines as 4 x 9 stages: ~85 registers, 24 warps per SM
-    FFT3D_TWOPASS_PFA36(3, 256, 3);
-    FFT3D_TWOPASS_PFA36(2, 256, 4);
-    FFT3D_TWOPASS_PFA36(4, 256, 2);
-    FFT3D_TWOPASS_PFA36(3, 384, 2);
-    FFT3D_TWOPASS_PFA36(2, 192, 5);
+    // 36-point lines as 4 x 9 stages (tuner candidates; one line per thread wins on B200)
+    FFT3D_TWOPASS_STAGED(LinePFA36, 36, double, "pfa", 128, 8);
+    FFT3D_TWOPASS_STAGED(LinePFA36, 36, float, "pfa", 128, 8);
     // z pass in shared memory, y and x passes between registers and L2
     FFT3D_TWOPASS_REGS(36, 36, 36, 3, 128, 3);
     FFT3D_TWOPASS_REGS(36, 36, 36, 2, 96, 4);

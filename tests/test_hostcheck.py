@@ -172,50 +172,6 @@ def test_twopass_lean_control_variants(hostcheck, shape, base, g, nvol, sign):
     assert oracle.rel_error_per_volume(got, want).max() < C128_TOL
 
 
-PFA = [(3, 7), (2, 11), (4, 3), (3, 1)]
-
-
-@pytest.mark.parametrize("g,nvol", PFA, ids=[f"g{t[0]}-b{t[1]}" for t in PFA])
-@pytest.mark.parametrize("sign", [-1, +1])
-def test_twopass_pfa36_stages(hostcheck, g, nvol, sign):
-    """36^3 TWOPASS with every line split into its 4 x 9 Good-Thomas stages
-    (alg = 600 + G): the index maps of pfa36.cuh, the in-place stage order and
-    the three pass layouts, in ticket order with the dependency check."""
-    import ctypes
-    hostcheck.hostcheck_twopass_violations.restype = ctypes.c_longlong
-    hostcheck.hostcheck_twopass_violations()
-    rng = np.random.default_rng(8000 + g + nvol)
-    x = field(rng, (nvol, 36, 36, 36), dist="normal")
-    got = run(hostcheck, x, (36, 36, 36), 0, sign, 600 + g, 1)
-    assert hostcheck.hostcheck_twopass_violations() == 0
-    want = oracle.fft3d(x) if sign < 0 else oracle.ifft3d(x)
-    assert oracle.rel_error_per_volume(got, want).max() < C128_TOL
-
-
-STAGED = [(64, 1, 0), (64, 3, 0), (64, 2, 1), (45, 3, 0), (45, 1, 0)]
-
-
-@pytest.mark.parametrize("n,nvol,prec", STAGED, ids=[f"{t[0]}-b{t[1]}-p{t[2]}" for t in STAGED])
-@pytest.mark.parametrize("sign", [-1, +1])
-def test_twopass_staged_lines(hostcheck, n, nvol, prec, sign):
-    """TWOPASS with every line split into two thread-level stages (alg = 701):
-    64 = 8 x 8 Cooley-Tukey and 45 = 5 x 9 Good-Thomas (staged.cuh) -- the
-    twiddles and index maps, the permuted in-place z pass and the natural-order
-    stores, both precisions' row pitches, in ticket order with the dependency
-    check."""
-    import ctypes
-    hostcheck.hostcheck_twopass_violations.restype = ctypes.c_longlong
-    hostcheck.hostcheck_twopass_violations()
-    rng = np.random.default_rng(9000 + n + nvol)
-    dt = np.complex128 if prec == 0 else np.complex64
-    x = field(rng, (nvol, n, n, n), dist="normal", dtype=dt)
-    got = run(hostcheck, x, (n, n, n), prec, sign, 701, 1)
-    assert hostcheck.hostcheck_twopass_violations() == 0
-    x64 = x.astype(np.complex128)
-    want = oracle.fft3d(x64) if sign < 0 else oracle.ifft3d(x64)
-    assert oracle.rel_error_per_volume(got, want).max() < (C128_TOL if prec == 0 else C64_TOL)
-
-
 SPLIT = [((36, 36, 36), 0, 2, 11), ((36, 36, 36), 0, 1, 3), ((36, 36, 36), 1, 4, 5),
          ((64, 64, 64), 0, 1, 3), ((64, 64, 64), 1, 2, 2), ((36, 36, 64), 0, 2, 4)]
 

@@ -73,7 +73,11 @@ void fft3d_b200_plan_destroy(fft3d_b200_plan *plan);
 /* Transform device-resident data on `stream` (a cudaStream_t; NULL = the legacy
  * default stream).  Asynchronous: returns once the work is enqueued.  `in` and
  * `out` must be distinct device buffers of batch*n0*n1*n2 elements aligned to the
- * element size. */
+ * element size.  On any stream but the legacy default one the kernel is launched
+ * with programmatic dependent launch: its CTAs may be placed while the previous
+ * kernel of the stream drains, and wait for that kernel to complete before their
+ * first global memory access (stream order is kept; FFT3D_B200_PDL=0 in the
+ * environment launches in plain stream order). */
 int fft3d_b200_execute(fft3d_b200_plan *plan, const void *d_in, void *d_out, void *stream);
 
 /* Transform host data: copies in, transforms, copies out, and returns when `out`

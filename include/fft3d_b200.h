@@ -289,9 +289,18 @@ void fft3d_b200_server_destroy(fft3d_b200_server *server);
  * route needs more scratch than the array holds); beyond these it returns
  * FFT3D_B200_ERR_BUDGET and enqueues nothing.  The first call on a device looks
  * up the array's device address (make it before any stream capture).  Calls
- * share the array and reset its ticket on their stream, so calls that overlap
- * on the GPU race: order them (one stream, or events). */
+ * share the array and reset its ticket on their stream: host threads calling
+ * on the same stream are serialised, but calls that overlap on the GPU
+ * (different streams) race, so order them (one stream, or events).  The
+ * descriptors are copied from the call's stack memory, so while `stream` is
+ * being captured the call returns FFT3D_B200_ERR_INVALID and enqueues nothing. */
 int fft3d_b200_batch_execute_noalloc(const fft3d_b200_segment *segs, int nseg, void *stream);
+
+/* Status of the allocation-free launches enqueued on `stream` -- no counterpart
+ * in the reference.  Synchronises `stream`; FFT3D_B200_ERR_CUDA if a launch
+ * failed, FFT3D_B200_ERR_TIMEOUT if the shared array's device error word is
+ * set, else FFT3D_B200_OK.  Allocates nothing. */
+int fft3d_b200_noalloc_check(void *stream);
 
 #ifdef __cplusplus
 }

@@ -23,8 +23,14 @@
 // device current) looks the address up with cudaGetSymbolAddress and caches it;
 // make that first call before any stream capture.  Every call reuses the same
 // array: it copies the call's descriptors in and resets the ticket to zero on
-// the caller's stream, so calls that overlap on the GPU (on different streams)
-// race on the array and must be ordered by the caller.
+// the caller's stream.  Host threads that call on the same stream are serialised
+// from the first copy to the launch, so each launch reads its own descriptors;
+// calls that overlap on the GPU (different streams) race on the array and must
+// be ordered by the caller.  The descriptors are copied from the caller's stack,
+// so a stream that is being captured is refused (FFT3D_B200_ERR_INVALID): a
+// replayed copy would read stack memory that no longer holds them.
+// fft3d_b200_noalloc_check synchronises a stream and reports the launch's
+// status and the array's device error word.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -51,7 +57,8 @@ struct NoAllocDevice {
     int grid = 0;
 };
 
-static std::mutex g_noalloc_mu;
+static std::mutex g_noalloc_mu;        // first-time set-up
+static std::mutex g_noalloc_enqueue_mu;  // descriptor copies through the launch
 static NoAllocDevice g_noalloc_dev[64];
 
 // Once per device, with the device current: the symbol's device address, the
@@ -117,6 +124,9 @@ extern "C" int fft3d_b200_batch_execute_noalloc(const fft3d_b200_segment *segs, 
                                        nullptr);
         if (kind < 0) return FFT3D_B200_ERR_UNSUPPORTED;
         if (big && s.batch > 0) return FFT3D_B200_ERR_BUDGET;  // needs per-CTA scratch
+        // before any product with the batch: a segment alone above the item
+        // limit is refused, so the sums and byte counts below cannot overflow
+        if (s.batch > (long long)NOALLOC_MAX_ITEMS * vpc[i]) return FFT3D_B200_ERR_BUDGET;
         const size_t eb = (size_t)element_bytes(s.precision);
         const size_t bytes = (size_t)s.batch * (size_t)ve * eb;
         if (s.batch > 0) {
@@ -149,10 +159,17 @@ extern "C" int fft3d_b200_batch_execute_noalloc(const fft3d_b200_segment *segs, 
 
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess) return FFT3D_B200_ERR_CUDA;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) {
+        cudaGetLastError();
+        return FFT3D_B200_ERR_INVALID;
+    }
+    if (cap != cudaStreamCaptureStatusNone) return FFT3D_B200_ERR_INVALID;
     NoAllocDevice nd;
     int st = noalloc_setup(device, &nd);
     if (st) return st;
-    cudaStream_t s = (cudaStream_t)stream;
+    std::lock_guard<std::mutex> enqueue_lock(g_noalloc_enqueue_mu);
     BatchItem *d_items = (BatchItem *)(nd.base + NOALLOC_ITEMS_OFF);
     BatchSeg *d_segs = (BatchSeg *)(nd.base + NOALLOC_SEGS_OFF);
     unsigned int *d_ticket = (unsigned int *)(nd.base + NOALLOC_TICKET_OFF);
@@ -214,4 +231,21 @@ extern "C" int fft3d_b200_batch_execute_noalloc(const fft3d_b200_segment *segs, 
                          (size_t)batch_kernel_smem(), s) != cudaSuccess)
         return FFT3D_B200_ERR_CUDA;
     return FFT3D_B200_OK;
+}
+
+extern "C" int fft3d_b200_noalloc_check(void *stream)
+{
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) return FFT3D_B200_ERR_CUDA;
+    NoAllocDevice nd;
+    const int st = noalloc_setup(device, &nd);
+    if (st) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return FFT3D_B200_ERR_CUDA;
+    int v = 0;
+    const int *d_err = (const int *)(nd.base + NOALLOC_ERR_OFF);
+    if (cudaMemcpyAsync(&v, d_err, sizeof v, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return FFT3D_B200_ERR_CUDA;
+    return v == 0 ? FFT3D_B200_OK : FFT3D_B200_ERR_TIMEOUT;
 }

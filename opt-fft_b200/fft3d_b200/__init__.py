@@ -99,6 +99,7 @@ EXPORTS = {
                      "fft3d_b200_batch_create",
                      "fft3d_b200_batch_execute", "fft3d_b200_batch_destroy",
                      "fft3d_b200_batch_describe", "fft3d_b200_batch_execute_noalloc",
+                     "fft3d_b200_noalloc_check",
                      "fft3d_b200_chain_create", "fft3d_b200_chain_run",
                      "fft3d_b200_chain_destroy",
                      "fft3d_b200_server_create", "fft3d_b200_server_submit",
@@ -165,6 +166,7 @@ def _load():
         "fft3d_b200_batch_destroy": ([vp], None),
         "fft3d_b200_batch_describe": ([vp], ctypes.c_char_p),
         "fft3d_b200_batch_execute_noalloc": ([ctypes.POINTER(Segment), i, vp], i),
+        "fft3d_b200_noalloc_check": ([vp], i),
         "fft3d_b200_chain_create": ([i, i, i, ll, i, i, vp, i, ctypes.POINTER(vp)], i),
         "fft3d_b200_chain_run": ([vp, vp, vp, ll, vp], i),
         "fft3d_b200_chain_destroy": ([vp], None),
@@ -396,6 +398,11 @@ def batch_execute_noalloc(segments, stream: int = 0):
     see fft3d_b200_batch_execute_noalloc in include/fft3d_b200.h for the limits."""
     _check(_lib.fft3d_b200_batch_execute_noalloc(_segments(segments), len(segments),
                                                  stream or None), "batch_execute_noalloc")
+
+
+def noalloc_check(stream: int = 0):
+    """Synchronise `stream` and raise if an allocation-free launch on it failed."""
+    _check(_lib.fft3d_b200_noalloc_check(stream or None), "noalloc_check")
 
 
 class Batch:

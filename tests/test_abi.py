@@ -92,3 +92,30 @@ def test_no_cpu_fallback_without_gpu():
     with pytest.raises(fb.Fft3dError) as e:
         fb.Batch([])
     assert e.value.status == fb.ERR_CUDA
+
+
+@pytest.mark.skipif(cuda_available(), reason="dummy device addresses: host-only check")
+def test_noalloc_limits_are_checked_on_the_host():
+    """The allocation-free batch refuses oversized requests before any CUDA
+    call: too many work items in total, one segment alone past the limit (a
+    batch whose item count would overflow a 64-bit sum), more segments than
+    descriptors.  The addresses are never dereferenced; without a GPU any
+    request that got past validation would fail with ERR_CUDA instead."""
+    lib = fb.lib()
+    a, b = 1 << 40, 1 << 44  # distinct, aligned, never touched
+    # 8^3 complex64 items hold 25 volumes: 16385 * 25 volumes make one item too many
+    one = {"shape": (8, 8, 8), "batch": 16385 * 25, "precision": fb.C64, "in": a, "out": b}
+    assert lib.fft3d_b200_batch_execute_noalloc(fb._segments([one]), 1, None) == fb.ERR_BUDGET
+    # two segments under the limit that exceed it together
+    half = dict(one, batch=8193 * 25)
+    half2 = dict(half, **{"in": a + (1 << 36), "out": b + (1 << 36)})
+    assert lib.fft3d_b200_batch_execute_noalloc(fb._segments([half, half2]), 2,
+                                                None) == fb.ERR_BUDGET
+    huge = dict(one, batch=(1 << 62) + 5)
+    assert lib.fft3d_b200_batch_execute_noalloc(fb._segments([huge]), 1, None) == fb.ERR_BUDGET
+    small = dict(one, batch=4)
+    assert lib.fft3d_b200_batch_execute_noalloc(fb._segments([small] * 257), 257,
+                                                None) == fb.ERR_BUDGET
+    # a request inside the limits passes validation and then meets the missing GPU
+    assert lib.fft3d_b200_batch_execute_noalloc(fb._segments([small]), 1, None) == fb.ERR_CUDA
+    assert lib.fft3d_b200_noalloc_check(None) == fb.ERR_CUDA

@@ -8,14 +8,14 @@ entry point keeps that scratch in a static device array instead.  This test
 calls it through the C ABI twice in a row (the second call reuses the array the
 first one left behind, ticket included) and checks each result against the
 allocating entry point, fft3d_b200_batch_create + fft3d_b200_batch_execute,
-within the parity tolerances of the other tests; it also checks that requests
-beyond the array's limits are refused with FFT3D_B200_ERR_BUDGET.
+and against the FP64 oracle (oracle/fft3d_oracle.c), within the parity
+tolerances of the other tests; fft3d_b200_noalloc_check reads each call's
+status.  It also checks that requests beyond the array's limits are refused
+with FFT3D_B200_ERR_BUDGET and that a capturing stream is refused.
 
 Kept in a file of its own that pytest collects last, so a stop-at-first-failure
 run has already run every other test.  It needs no state from other tests.
 """
-import ctypes
-
 import numpy as np
 import pytest
 
@@ -23,17 +23,10 @@ torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
 import fft3d_b200 as fb  # noqa: E402
+import oracle  # noqa: E402
 
-C128_TOL = 1e-13
-C64_TOL = 2e-6
-
-
-def rel_err_per_volume(a, b):
-    a = a.reshape(a.shape[0], -1).astype(np.complex128)
-    b = b.reshape(b.shape[0], -1).astype(np.complex128)
-    den = np.linalg.norm(b, axis=1)
-    den[den == 0] = 1.0
-    return np.linalg.norm(a - b, axis=1) / den
+C128_TOL = 1e-13  # relative L2 per volume against the FP64 oracle
+C64_TOL = 1e-6    # complex64 (FP32 arithmetic) against the FP64 oracle
 
 
 def _segments(rng):
@@ -56,9 +49,19 @@ def _seg_dicts(specs, outs):
             for (s, n, p, d, x), o in zip(specs, outs)]
 
 
-def test_noalloc_matches_allocating_batch_twice():
+def _expected(specs):
+    """FP64 oracle of every segment, from the exact inputs the GPU reads."""
+    out = []
+    for shape, n, prec, d, x in specs:
+        xin = x.cpu().numpy().astype(np.complex128)
+        out.append(oracle.fft3d(xin) if d == fb.FORWARD else oracle.ifft3d(xin))
+    return out
+
+
+def test_noalloc_matches_allocating_batch_and_oracle_twice():
     rng = np.random.default_rng(31)
     specs = _segments(rng)
+    want = _expected(specs)
     ref_outs = [torch.empty_like(x) for *_, x in specs]
     ref = fb.Batch(_seg_dicts(specs, ref_outs))
     ref.execute()
@@ -68,16 +71,20 @@ def test_noalloc_matches_allocating_batch_twice():
         outs = [torch.full_like(x, complex(7.0, -7.0)) for *_, x in specs]
         arr = fb._segments(_seg_dicts(specs, outs))
         st = lib.fft3d_b200_batch_execute_noalloc(arr, len(specs), None)
-        assert st == fb.OK, fb.lib().fft3d_b200_status_string(st)
-        torch.cuda.synchronize()
-        for (shape, n, prec, d, x), o, r in zip(specs, outs, ref_outs):
-            err = rel_err_per_volume(o.cpu().numpy(), r.cpu().numpy())
+        assert st == fb.OK, lib.fft3d_b200_status_string(st)
+        assert lib.fft3d_b200_noalloc_check(None) == fb.OK
+        for (shape, n, prec, d, x), o, r, w in zip(specs, outs, ref_outs, want):
+            got = o.cpu().numpy()
             tol = C128_TOL if prec == fb.C128 else C64_TOL
-            assert err.max() < tol, (call, shape, prec, d, err.max())
+            e_ref = oracle.rel_error_per_volume(got, r.cpu().numpy())
+            e_orc = oracle.rel_error_per_volume(got, w)
+            assert e_ref.max() < tol, (call, shape, prec, d, "vs batch", e_ref.max())
+            assert e_orc.max() < tol, (call, shape, prec, d, "vs oracle", e_orc.max())
     ref.close()
 
 
 def test_noalloc_refuses_requests_beyond_its_array():
+    """Refusals decided on the host before anything is enqueued (small buffers)."""
     lib = fb.lib()
     x = torch.zeros(16 * 512, dtype=torch.complex128, device="cuda")
     y = torch.zeros_like(x)
@@ -85,15 +92,6 @@ def test_noalloc_refuses_requests_beyond_its_array():
     # more segments than the array has descriptors for
     arr = fb._segments([one] * 257)
     assert lib.fft3d_b200_batch_execute_noalloc(arr, 257, None) == fb.ERR_BUDGET
-    # more work items than it has room for: 8^3 complex64 items hold 25 volumes,
-    # so 16385 * 25 volumes make 16385 items, one more than the limit
-    nbig = 16385 * 25
-    big = torch.zeros(nbig * 512, dtype=torch.complex64, device="cuda")
-    out = torch.zeros_like(big)
-    arr = fb._segments([{"shape": (8, 8, 8), "batch": nbig, "precision": fb.C64,
-                         "in": big.data_ptr(), "out": out.data_ptr()}])
-    assert lib.fft3d_b200_batch_execute_noalloc(arr, 1, None) == fb.ERR_BUDGET
-    del big, out
     # 36^3 needs per-CTA scratch the array does not hold
     c = torch.zeros(36 ** 3, dtype=torch.complex128, device="cuda")
     d = torch.zeros_like(c)
@@ -102,4 +100,24 @@ def test_noalloc_refuses_requests_beyond_its_array():
     assert lib.fft3d_b200_batch_execute_noalloc(arr, 1, None) == fb.ERR_BUDGET
     # an empty call is valid and enqueues nothing harmful
     assert lib.fft3d_b200_batch_execute_noalloc(fb._segments([]), 0, None) == fb.OK
+    assert lib.fft3d_b200_noalloc_check(None) == fb.OK
+
+
+def test_noalloc_refuses_a_capturing_stream():
+    """Its descriptor copies come from stack memory, so capture is refused."""
+    lib = fb.lib()
+    x = torch.zeros(4 * 512, dtype=torch.complex128, device="cuda")
+    y = torch.zeros_like(x)
+    arr = fb._segments([{"shape": (8, 8, 8), "batch": 4, "in": x.data_ptr(),
+                         "out": y.data_ptr()}])
+    s = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    sts = []
+    with torch.cuda.graph(g, stream=s):
+        sts.append(lib.fft3d_b200_batch_execute_noalloc(arr, 1, s.cuda_stream))
+        y.add_(0)  # keep the captured graph non-empty
+    assert sts == [fb.ERR_INVALID]
+    del g
     torch.cuda.synchronize()
+    assert lib.fft3d_b200_batch_execute_noalloc(arr, 1, None) == fb.OK
+    assert lib.fft3d_b200_noalloc_check(None) == fb.OK

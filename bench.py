@@ -11,12 +11,18 @@ included (`e2e`).  `roofline` describes the forward 17^3 kernel: algorithmic
 bytes (read + write once, 2*16*4913 B per volume) over its CUDA-event time,
 against the measured HBM copy bandwidth.  `workloads` adds the same per-L
 measurement (volumes/s, fraction of HBM roofline) for the other plain
-configurations.  `cpu_baseline` is the reference's best single-core C kernels
-(bench/geom/best, built into oracle/_ref) on a bounded sample, all host threads.
+configurations, the uneven complex64 batch, chains, the serving stream and a
+cuFFT library comparison (torch.fft on the same buffers; never called by the
+library).  `cpu_baseline` is the reference's own CPU code for the path, timed on
+this host (oracle/_ref): its best C kernels and textbook exemplar and FFTW
+3.3.10 built from its vendored source, single-thread and all host threads, each
+leg listed; the headline value is the fastest all-threads leg.  `per_l` (last)
+is a compact table: workload -> [volumes/s, fraction of HBM roofline, kernel].
 
 For N > 1 (torchrun, one rank per GPU) every rank transforms its own 2048
 volumes (weak scaling, no collective on the data path); time is the max over
-ranks.
+ranks.  `--impl reference` times the reference's best C kernels on all host
+threads over the full per-GPU batch (rank 0 only).
 """
 from __future__ import annotations
 
@@ -406,46 +412,81 @@ def measure_mixed(fb, torch, device, stream, peak, steps, warmup, world):
 
 # ------------------------------------------------------------------ serving
 
-def measure_serve(fb, torch, device, n_req=10000, seed=2024):
-    """Continuous-batching server vs one launch per request in FP64, on the seeded
-    serving stream: saturation throughput, then Poisson arrivals at 70% of the
-    batched saturation rate, with p50/p99 submit-to-completion latency.
-    Request data is device-resident and distinct per request (its own input and
-    output ranges of an arena larger than L2), so every request is served from
-    HBM; the FP64 baseline gets the same requests in complex128."""
-    from fft3d_b200.workloads import SIDES, request_stream
-    reqs = request_stream(n_req, rate_hz=1.0, seed=seed)
-    sizes =[r["batch"] * int(np.prod(r["shape"])) for r in reqs]
-    off = np.concatenate([[0], np.cumsum(sizes)])
-    total = int(off[-1])
-    a128 = torch.empty(total, dtype=torch.complex128, device=device)
-    a128.real.uniform_(-1, 1)
-    a128.imag.uniform_(-1, 1)
-    o128 = torch.empty_like(a128)
-    a64 = a128.to(torch.complex64)
-    o64 = torch.empty_like(a64)
+def measure_serve(fb, torch, device, n_req=1_000_000, seed=2024, arena_gb=(24, 4)):
+    """The serving configuration: a seeded stream of `n_req` requests through the
+    continuous-batching server, against one launch per request in FP64.
 
-    def seg_of(r, p, k):
-        src, dst = (a128, o128) if p == 0 else (a64, o64)
-        eb = 16 if p == 0 else 8
-        return {"shape": r["shape"], "batch": r["batch"], "direction": r["direction"],
-                "precision": p, "in": src.data_ptr() + int(off[k]) * eb,
-                "out": dst.data_ptr() + int(off[k]) * eb}
+    Request data is device-resident.  The stream (about 1 TB of input at 1e6
+    requests) cycles through rotating arenas well above L2 -- `arena_gb` GB of
+    input and as much of output for complex128 and for complex64 -- so every
+    request is read from and written to HBM; the FP64 baseline gets the same
+    requests in complex128.  Runs: saturation (everything queued at once), then
+    Poisson arrivals at 70% of the batched saturation rate; the baseline at that
+    same rate and at 70% of its own saturation rate.  p50/p99 are taken over the
+    steady-state window (requests 1%..99% of the stream by submission order)."""
+    from fft3d_b200.workloads import SIDES, arena_offsets, request_arrays
+    ra = request_arrays(n_req, rate_hz=1.0, seed=seed)
+    side, nvol = ra["side"], ra["batch"]
+    prec, direc = ra["precision"], ra["direction"]
+    pts = nvol * side ** 3
+    arena = {0: int(arena_gb[0]) << 30, 1: int(arena_gb[1]) << 30}
+    buf = {}
+    for p, dt in ((0, torch.float64), (1, torch.float32)):
+        eb = 8 if p == 0 else 4
+        x = torch.empty(arena[p] // eb, dtype=dt, device=device)
+        x.uniform_(-1.0, 1.0)
+        buf[p] = (x, torch.empty_like(x))
+
+    layouts = {}
+
+    def layout(force_c128):
+        if force_c128 in layouts:
+            return layouts[force_c128]
+        segs = np.zeros(n_req, dtype=fb.segment_dtype())
+        segs["n0"] = segs["n1"] = segs["n2"] = side
+        segs["direction"] = direc
+        segs["batch"] = nvol
+        p_of = np.zeros(n_req, dtype=np.int64) if force_c128 else prec
+        segs["precision"] = p_of
+        for p in (0, 1):
+            sel = np.nonzero(p_of == p)[0]
+            if not len(sel):
+                continue
+            nbytes = pts[sel] * (16 if p == 0 else 8)
+            off = arena_offsets(nbytes, arena[p])
+            segs["in_"][sel] = buf[p][0].data_ptr() + off
+            segs["out"][sel] = buf[p][1].data_ptr() + off
+        layouts[force_c128] = (segs, int((pts * np.where(p_of == 0, 16, 8)).sum()))
+        return layouts[force_c128]
 
     def run(flags, rate, force_c128, inflight):
-        # requests are submitted by the library's C load generator at their
-        # arrival times, so the client is never the bottleneck
-        srv = fb.Server(64 << 30, max_inflight=inflight, flags=flags)
-        segs = [seg_of(r, 0 if force_c128 else r["precision"], k) for k, r in enumerate(reqs)]
+        segs, nbytes = layout(force_c128)
         arrivals = None
         if rate:
-            gaps = np.random.default_rng(seed + 2).exponential(1.0 / rate, len(reqs))
+            gaps = np.random.default_rng(seed + 2).exponential(1.0 / rate, n_req)
             arrivals = np.cumsum(gaps) - gaps[0]
-        srv.submit_many(segs, arrivals)
-        srv.drain(600)
+        srv = fb.Server(64 << 30, max_inflight=inflight, flags=flags)
+        tk = srv.submit_array(segs, arrivals)
+        srv.drain(1800)
         st = srv.stats()
+        done_tk, lat = srv.latencies()
         srv.close()
-        return st
+        # steady-state window by submission order (tickets are 1..n in order)
+        first = int(tk[0])
+        idx = done_tk.astype(np.int64) - first
+        keep = (idx >= n_req // 100) & (idx < n_req - n_req // 100)
+        w = lat[keep]
+        out = {"volumes_per_s": st["volumes_per_s"], "requests_per_s": st["requests"] / st["span_s"],
+               "p50_s": float(np.percentile(w, 50)), "p99_s": float(np.percentile(w, 99)),
+               "p50_all_s": st["p50_s"], "p99_all_s": st["p99_s"], "max_s": st["max_s"],
+               "mean_requests_per_launch": st["mean_requests_per_launch"], "launches": st["launches"],
+               "span_s": st["span_s"], "peak_admitted_bytes": st["peak_admitted_bytes"],
+               "steady_window_requests": int(keep.sum()), "bytes_in": nbytes}
+        if rate:
+            out["arrival_rate_hz"] = rate
+            # keeps up: finished within 10% of the arrival span
+            out["keeps_up"] = bool(st["span_s"] < 1.1 * float(arrivals[-1]) + 0.05)
+        return out
 
     # warm-up: every kind and volume-count class once (tuning, first launches)
     warm = []
@@ -453,31 +494,31 @@ def measure_serve(fb, torch, device, n_req=10000, seed=2024):
         for d in (-1, 1):
             for p in (0, 1):
                 for b in (1, 2, 4, 8, 16, 32, 64):
-                    warm.append({"shape": (L, L, L), "batch": b, "direction": d, "precision": p})
+                    warm.append((L, d, p, b))
     for flags, inflight in ((0, 4), (fb.SERVE_PLAIN, 32)):
         srv = fb.Server(64 << 30, max_inflight=inflight, flags=flags)
-        for k, r in enumerate(warm):
-            srv.submit(seg_of(r, r["precision"], k))
+        for L, d, p, b in warm:
+            srv.submit({"shape": (L, L, L), "batch": b, "direction": d, "precision": p,
+                        "in": buf[p][0].data_ptr(), "out": buf[p][1].data_ptr()})
         srv.drain(600)
         srv.close()
     torch.cuda.synchronize()
 
-    out = {"label": f"{n_req} requests of the seeded serving stream, device-resident data, "
-                    "64 GB admission budget"}
+    out = {"label": f"{n_req} requests of the seeded serving stream (Poisson arrivals, 1-64 volumes, "
+                    "L in {6..36} p~1/L, fwd/inv 50/50, c128 75%), device-resident data in rotating "
+                    f"arenas of {arena_gb[0]}+{arena_gb[0]} GB (c128) and {arena_gb[1]}+{arena_gb[1]} GB "
+                    "(c64), 64 GB admission budget; p50/p99 over requests 1%..99% of the stream",
+           "n_requests": n_req}
     sat = run(0, None, False, 4)
-    lam = 0.7 * sat["requests"] / sat["span_s"]
-    pois = run(0, lam, False, 4)
+    lam = 0.7 * sat["requests_per_s"]
+    out["batched_saturation"] = sat
+    out["batched_poisson"] = run(0, lam, False, 4)
     psat = run(fb.SERVE_PLAIN, None, True, 32)
-    ppois = run(fb.SERVE_PLAIN, lam, True, 32)
-    keep = ("volumes_per_s", "p50_s", "p99_s", "mean_requests_per_launch", "launches")
-    out["batched_saturation"] = {k: sat[k] for k in keep}
-    out["batched_poisson"] = dict({k: pois[k] for k in keep}, arrival_rate_hz=lam)
-    out["plain_fp64_saturation"] = {k: psat[k] for k in keep}
-    out["plain_fp64_poisson"] = dict({k: ppois[k] for k in keep}, arrival_rate_hz=lam)
+    out["plain_fp64_saturation"] = psat
+    out["plain_fp64_poisson_same_rate"] = run(fb.SERVE_PLAIN, lam, True, 32)
+    out["plain_fp64_poisson_own_rate"] = run(fb.SERVE_PLAIN, 0.7 * psat["requests_per_s"], True, 32)
     out["throughput_ratio_saturation"] = sat["volumes_per_s"] / psat["volumes_per_s"]
-    out["bytes_in_per_run"] = int(sum(s * (16 if r["precision"] == 0 else 8)
-                                      for s, r in zip(sizes, reqs)))
-    del a128, o128, a64, o64
+    del buf
     return out
 
 
@@ -547,60 +588,256 @@ def aligned(shape, dtype=np.complex128, align=64):
     return buf[off:off + n].view(dtype).reshape(shape)
 
 
-def cpu_reference(name, seconds=10.0, threads=None, max_sample=None):
-    """The reference's own C kernels (oracle/_ref) when built, else the oracle port.
-    Returns (volumes/s, kind, threads, sample description, per-run seconds)."""
-    w = WORKLOADS[name]
-    L = w["shape"][0]
-    roundtrip = len(w["chain"]) == 2
-    threads = threads or os.cpu_count() or 1
-    lib_path = os.path.join(ROOT, "oracle", "_ref", "libfft3d_best.so")
-    vol = int(np.prod(w["shape"]))
-    sample = max_sample or max(threads * 4, min(w["batch"], (64 << 20) // (vol * 16)))
-    sample = min(sample, w["batch"])
-    rng = np.random.default_rng(99)
-    x = aligned((sample,) + w["shape"])
-    x[:] = field(rng, (sample,) + w["shape"], w["dist"], np.complex128)
-    out = aligned((sample,) + w["shape"])
-    if os.path.exists(lib_path) and w["prec"] == 0 and w["shape"][0] == w["shape"][1] == w["shape"][2]:
-        lib = ctypes.CDLL(lib_path)
-        lib.ref_create.restype = ctypes.c_void_p
-        lib.ref_create.argtypes = [ctypes.c_int, ctypes.c_long, ctypes.c_int, ctypes.c_int]
+REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libfft3d_best.so")
+REF_BEST, REF_TEXTBOOK, REF_FFTW, REF_FFTW_THREADS = 0, 1, 2, 3
+_REF = []
+
+
+def ref_lib():
+    """oracle/_ref/libfft3d_best.so: the reference's CPU code behind ref_shim.c."""
+    if not _REF:
+        if not os.path.exists(REF_LIB):
+            return None
+        lib = ctypes.CDLL(REF_LIB)
+        lib.ref_open.restype = ctypes.c_void_p
+        lib.ref_open.argtypes = [ctypes.c_int] * 4 + [ctypes.c_long] + [ctypes.c_int] * 4
         lib.ref_run.argtypes = [ctypes.c_void_p] * 3
         lib.ref_destroy.argtypes = [ctypes.c_void_p]
         lib.ref_kernel_name.argtypes = [ctypes.c_void_p]
         lib.ref_kernel_name.restype = ctypes.c_char_p
-        ctx = lib.ref_create(L, sample, threads, 1 if roundtrip else 0)
-        run = lambda: lib.ref_run(ctx, x.ctypes.data, out.ctypes.data)  # noqa: E731
-        kind = "reference"
-        kname = lib.ref_kernel_name(ctx).decode()
-        desc = (f"bench/geom/best {kname} (reference C, -march=sapphirerapids), "
-                f"{sample} volumes per run{', inverse by conjugation' if roundtrip else ''}")
-    else:
-        import oracle
-        ctx = None
+        lib.ref_threads.argtypes = [ctypes.c_void_p]
+        lib.ref_plan_seconds.argtypes = [ctypes.c_void_p]
+        lib.ref_plan_seconds.restype = ctypes.c_double
+        _REF.append(lib)
+    return _REF[0]
 
-        def run():
-            y = oracle.fft3d(x, nthreads=threads)
-            if roundtrip:
-                oracle.ifft3d(y, nthreads=threads)
-        kind = "port"
-        desc = f"oracle/fft3d_oracle.c restatement, {sample} volumes per run"
-    run()  # first touch
-    runs, t0 = 0, time.perf_counter()
-    while True:
-        run()
-        runs += 1
-        el = time.perf_counter() - t0
-        if el >= seconds:
-            break
-    per = el / runs
-    if ctx:
-        lib.ref_destroy(ctx)
-    return sample / per, kind, threads, desc + f", {runs} runs over {el:.1f} s", per
+
+def host_info():
+    """CPU model, ISA and thread count of this host (as bench/geom/sweep.sh:28-35 records)."""
+    model, flags = None, set()
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name") and model is None:
+                model = line.split(":", 1)[1].strip()
+            elif line.startswith("flags") and not flags:
+                flags = set(line.split(":", 1)[1].split())
+            if model and flags:
+                break
+    except OSError:
+        pass
+    isa = [f for f in ("sse4_2", "avx2", "fma", "avx512f", "avx512dq", "avx512vl", "avx512_fp16",
+                       "amx_tile") if f in flags]
+    return {"cpu_model": model, "isa": isa, "nproc": os.cpu_count(),
+            "threads_available": len(os.sched_getaffinity(0))}
+
+
+class RefLeg:
+    """One CPU leg: a reference backend planned once for a fixed batch, its
+    threads parked between runs (oracle/ref_shim.c)."""
+
+    def __init__(self, backend, shape, batch, prec, threads, roundtrip, effort=0, dist="uniform"):
+        lib = ref_lib()
+        self.lib = lib
+        self.batch = batch
+        self.ctx = lib.ref_open(backend, shape[0], shape[1], shape[2], batch, prec, threads,
+                                1 if roundtrip else 0, effort) if lib else None
+        if not self.ctx:
+            raise RuntimeError(f"reference backend {backend} cannot plan {shape} x{batch}")
+        dt = np.complex64 if prec else np.complex128
+        self.x = aligned((batch,) + tuple(shape), dt)
+        self.x[...] = field(np.random.default_rng(99), (batch,) + tuple(shape), dist, dt)
+        self.out = aligned((batch,) + tuple(shape), dt)
+        self.name = lib.ref_kernel_name(self.ctx).decode()
+        self.threads = lib.ref_threads(self.ctx)
+        self.plan_s = lib.ref_plan_seconds(self.ctx)
+
+    def run(self):
+        self.lib.ref_run(self.ctx, self.x.ctypes.data, self.out.ctypes.data)
+
+    def timed(self, seconds=0.0, runs=None):
+        """Volumes/s over a loop of `runs` runs, or of at least `seconds` (>= 3 runs),
+        after one untimed run."""
+        self.run()
+        n, t0 = 0, time.perf_counter()
+        while True:
+            self.run()
+            n += 1
+            el = time.perf_counter() - t0
+            if (runs is not None and n >= runs) or (runs is None and el >= seconds and n >= 3):
+                break
+        return self.batch * n / el, n, el
+
+    def close(self):
+        if self.ctx:
+            self.lib.ref_destroy(self.ctx)
+            self.ctx = None
+
+
+def cpu_legs(name, seconds, threads, full=True):
+    """Every CPU leg for a workload.  Single-thread legs run a bounded sample of
+    the batch; all-threads legs the whole batch.  The reference kernels are
+    complex128 cubes, forward only: their inverse is taken by conjugation.
+    FFTW legs run FFTW_BACKWARD + 1/V for the inverse, and are the labelled
+    stand-in where the reference has no C kernel (anisotropic, complex64)."""
+    w = WORKLOADS[name]
+    shape, batch, prec = w["shape"], w["batch"], w["prec"]
+    roundtrip = len(w["chain"]) == 2
+    vol = int(np.prod(shape))
+    eb = 16 if prec == 0 else 8
+    one = max(8, min(batch, (8 << 20) // (vol * eb)))
+    tb = max(2, min(batch, (1 << 20) // (vol * eb)))
+    cube = shape[0] == shape[1] == shape[2]
+    specs = []
+    if cube and prec == 0:
+        specs += [("best C, 1 thread", REF_BEST, 1, one, 0),
+                  ("best C, all threads", REF_BEST, threads, batch, 0)]
+        if full:
+            specs.append(("textbook C, 1 thread", REF_TEXTBOOK, 1, tb, 0))
+    if full:
+        specs += [(f"FFTW {e}, 1 thread", REF_FFTW, 1, one, k)
+                  for k, e in enumerate(("estimate", "measure", "patient"))]
+        specs.append(("FFTW measure, one plan per thread slice, all threads", REF_FFTW, threads, batch, 1))
+    specs.append(("FFTW measure, fftw_plan_with_nthreads, all threads", REF_FFTW_THREADS, threads, batch, 1))
+    legs = []
+    for label, backend, thr, n, effort in specs:
+        try:
+            leg = RefLeg(backend, shape, n, prec, thr, roundtrip, effort, w["dist"])
+        except RuntimeError as e:
+            legs.append({"leg": label, "error": str(e)})
+            continue
+        v, runs, el = leg.timed(seconds)
+        inv = ""
+        if roundtrip:
+            inv = ("; inverse by FFTW_BACKWARD + 1/V" if backend >= REF_FFTW
+                   else "; inverse by conjugation of the forward kernel")
+        legs.append({"leg": label, "value": v, "unit": "volumes/s", "threads": leg.threads,
+                     "impl": leg.name + inv, "sample_volumes": n, "runs": runs,
+                     "seconds": round(el, 3), "plan_s": round(leg.plan_s, 3)})
+        leg.close()
+    return legs
+
+
+def cpu_baseline(name, seconds, threads):
+    """The fastest all-threads leg as the headline CPU baseline, every leg listed."""
+    if ref_lib() is None:
+        return None
+    legs = cpu_legs(name, seconds, threads)
+    allc = [g for g in legs if "value" in g and g["threads"] > 1] or [g for g in legs if "value" in g]
+    if not allc:
+        return None
+    best = max(allc, key=lambda g: g["value"])
+    return {"value": best["value"], "unit": "volumes/s", "cores": best["threads"], "kind": "reference",
+            "sample": (f"{best['leg']}: {best['impl']}, {best['sample_volumes']} volumes per run, "
+                       f"{best['runs']} runs over {best['seconds']} s"),
+            "legs": legs, "host": host_info()}
+
+
+# ------------------------------------------------------------------ cuFFT (library comparison)
+
+class TorchFFT:
+    """torch.fft.fftn / ifftn (cuFFT) over a workload's rotating buffers: a
+    library comparison only, never called by the library."""
+
+    def __init__(self, torch, wl):
+        self.torch, self.wl = torch, wl
+        self.it = 0
+
+    def step(self, stream):
+        bufs = self.wl.sets[self.it % self.wl.nsets]
+        self.it += 1
+        for k, d in enumerate(self.wl.w["chain"]):
+            fn = self.torch.fft.fftn if d < 0 else self.torch.fft.ifftn
+            fn(bufs[k], dim=(-3, -2, -1), out=bufs[k + 1])
+
+    def launches_per_step(self):
+        return len(self.wl.w["chain"])
+
+
+def measure_cufft(torch, wl, stream, steps, warmup, peak):
+    try:
+        with torch.cuda.stream(stream):
+            ms, per_call, _ = time_device(torch, TorchFFT(torch, wl), stream, steps, warmup)
+        how = "graph-captured"
+    except Exception as e:  # cuFFT calls that cannot be captured: time them eagerly
+        torch.cuda.synchronize()
+        t = TorchFFT(torch, wl)
+        with torch.cuda.stream(stream):
+            for _ in range(warmup):
+                t.step(stream)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                t.step(stream)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        per_call = ms / t.launches_per_step()
+        how = f"eager ({type(e).__name__})"
+    ach = 2 * wl.bytes / (per_call * 1e-3) / 1e9
+    return {"volumes_per_s": wl.batch / (ms * 1e-3), "ms_per_step": ms, "achieved_gbs": ach,
+            "frac": ach / peak, "timing": how}
 
 
 # ------------------------------------------------------------------ main
+
+def make_config(name, world, nsets=None):
+    """The config block both arms report, so that they compare like with like."""
+    w = WORKLOADS[name]
+    vol = int(np.prod(w["shape"]))
+    bytes_ = w["batch"] * vol * (16 if w["prec"] == 0 else 8)
+    if nsets is None:
+        nsets = max(1, -(-3 * L2_BYTES // (bytes_ * (len(w["chain"]) + 1))))
+    return {"workload": name, "shape": list(w["shape"]), "global_batch": world * w["batch"],
+            "per_gpu_batch": w["batch"], "precision": "c128" if w["prec"] == 0 else "c64",
+            "step": "forward+inverse" if len(w["chain"]) == 2 else "forward",
+            "l2": (f"inputs larger than L2 ({bytes_ / 2**20:.0f} MiB per buffer, "
+                   f"{nsets} rotating buffer sets)"),
+            "parallelism": f"dp{world} (volumes sharded, no collective)"}
+
+
+def reference_arm(a, world, rank, metric):
+    """--impl reference: the reference's best C kernels (bench/geom/best) on every
+    host thread over the full per-GPU batch, planned once, threads parked between
+    steps; W untimed steps, then K timed steps.  FFTW with its own threads where
+    the reference has no C kernel (anisotropic, complex64)."""
+    if rank != 0:
+        return
+    w = WORKLOADS[a.workload]
+    threads = len(os.sched_getaffinity(0))
+    roundtrip = len(w["chain"]) == 2
+    cube = w["shape"][0] == w["shape"][1] == w["shape"][2]
+    backend = REF_BEST if (cube and w["prec"] == 0) else REF_FFTW_THREADS
+    if ref_lib() is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libfft3d_best.so was not built"}))
+        return
+    leg = RefLeg(backend, w["shape"], w["batch"], w["prec"], threads, roundtrip,
+                 effort=1, dist=w["dist"])
+    for _ in range(a.warmup):
+        leg.run()
+    times = []
+    for _ in range(a.steps):
+        t0 = time.perf_counter()
+        leg.run()
+        times.append(time.perf_counter() - t0)
+    per = sum(times) / len(times)
+    value = w["batch"] / per
+    inv = ("; inverse by conjugation of the forward kernel" if backend == REF_BEST
+           else "; inverse by FFTW_BACKWARD + 1/V") if roundtrip else ""
+    desc = (f"{leg.name}{inv}; {w['batch']} volumes per step (the per-GPU batch), {leg.threads} host "
+            f"threads parked between steps, planned once ({leg.plan_s:.1f} s, untimed)")
+    leg.close()
+    line = {"impl": "reference", "metric": metric, "value": value, "unit": "volumes/s",
+            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": per * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if w["prec"] == 0 else "f32", "data": "synthetic",
+            "config": make_config(a.workload, world),
+            "cpu_baseline": {"value": value, "unit": "volumes/s", "cores": threads, "kind": "reference",
+                             "sample": desc, "host": host_info()},
+            "e2e": {"value": value, "unit": "volumes/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
 
 def main():
     ap = argparse.ArgumentParser()
@@ -611,10 +848,11 @@ def main():
     ap.add_argument("--workload", default="roundtrip17", choices=sorted(WORKLOADS))
     ap.add_argument("--no-extra", action="store_true", help="skip the per-L workloads")
     ap.add_argument("--extras", default="all",
-                    help="comma list of the per-L workloads to run (default all, incl. mixed_c64; "
-                         "f4: the 13, 23, 45, 64 extents in both precisions)")
-    ap.add_argument("--cpu-seconds", type=float, default=10.0,
-                    help="CPU baseline sample length; 0 skips it")
+                    help="comma list of the per-L workloads to run (default all, incl. mixed_c64, "
+                         "chain, serve, cufft; f4: the 13, 23, 45, 64 extents in both precisions)")
+    ap.add_argument("--cpu-seconds", type=float, default=2.0,
+                    help="seconds per CPU baseline leg; 0 skips the CPU baseline")
+    ap.add_argument("--serve-requests", type=int, default=1_000_000)
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-pointer measurement")
     ap.add_argument("--variant", default=None,
                     help="force this kernel variant for the headline plans (profiling)")
@@ -628,28 +866,7 @@ def main():
     metric = f"volumes/s ({w['label']})"
 
     if a.impl == "reference":
-        if rank != 0:
-            return
-        vps = []
-        per_step = None
-        for _ in range(a.warmup):
-            cpu_reference(a.workload, seconds=0.0)
-        for _ in range(a.steps):
-            v, kind, thr, desc, per_step = cpu_reference(a.workload, seconds=0.0)
-            vps.append(v)
-        value = statistics.median(vps)
-        line = {"impl": "reference", "metric": metric, "value": value, "unit": "volumes/s",
-                "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
-                "ms_per_step": per_step * 1e3, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": a.workload, "shape": list(w["shape"]),
-                           "global_batch": w["batch"], "precision": "c128",
-                           "step": "forward+inverse" if len(w["chain"]) == 2 else "forward"},
-                "cpu_baseline": {"value": value, "unit": "volumes/s", "cores": thr, "kind": kind,
-                                 "sample": desc},
-                "e2e": {"value": value, "unit": "volumes/s", "h2d_bytes_per_step": 0,
-                        "d2h_bytes_per_step": 0}}
-        print(json.dumps(line))
+        reference_arm(a, world, rank, metric)
         return
 
     import torch
@@ -692,8 +909,15 @@ def main():
                "path": "fft3d_b200_execute_host_chain, page-locked host buffers"}
 
     workloads = {}
-    extras = (EXTRA + ["mixed_c64", "chain", "serve"] if a.extras == "all"
+    per_l = {a.workload: [value, roofline["frac"], roofline["kernel"]]}
+    extras = (EXTRA + ["mixed_c64", "chain", "serve", "cufft"] if a.extras == "all"
               else F4 if a.extras == "f4" else [e for e in a.extras.split(",") if e])
+    cufft = {}
+    if not a.no_extra and "cufft" in extras:
+        cufft[a.workload] = measure_cufft(torch, wl, stream, max(5, a.steps // 2), a.warmup, peak)
+    launches_per_step = wl.launches_per_step()
+    del wl
+    torch.cuda.empty_cache()
     if not a.no_extra:
         for name in extras:
             if name not in WORKLOADS:
@@ -712,39 +936,67 @@ def main():
                                "copy_same_bytes_gbs": cfx, "frac_of_copy_same_bytes": ach / cfx,
                                "kernel": x.plans[0].describe(),
                                "traffic": traffic.get(name)}
+            per_l[name] = [workloads[name]["volumes_per_s"], ach / peak, workloads[name]["kernel"]]
+            if "cufft" in extras:
+                cufft[name] = measure_cufft(torch, x, stream, max(5, a.steps // 2), a.warmup, peak)
+                cufft[name]["ours_over_cufft"] = workloads[name]["volumes_per_s"] / world / \
+                    cufft[name]["volumes_per_s"]
+            if rank == 0 and world == 1 and a.cpu_seconds > 0 and ref_lib() is not None:
+                workloads[name]["cpu_all_threads"] = cpu_legs(
+                    name, min(a.cpu_seconds, 1.0), len(os.sched_getaffinity(0)), full=False)
             del x
             torch.cuda.empty_cache()
+    if cufft:
+        if a.workload in cufft:
+            cufft[a.workload]["ours_over_cufft"] = value / world / cufft[a.workload]["volumes_per_s"]
+        workloads["cufft_library_comparison"] = dict(
+            {"label": "torch.fft.fftn/ifftn (cuFFT) on the same buffers, graph-captured like ours; "
+                      "a library comparison only, never called by the library"}, **cufft)
 
     if not a.no_extra and "mixed_c64" in extras:
         workloads["mixed_c64"] = measure_mixed(fb, torch, device, stream, peak, max(5, a.steps // 20),
                                                a.warmup, world)
+        mx = workloads["mixed_c64"]
+        per_l["mixed_c64"] = [mx["batch_volumes_per_s"], mx["frac"], "batch (autotuned)"]
         torch.cuda.empty_cache()
     if not a.no_extra and "chain" in extras:
         workloads["chain"] = measure_chain(fb, torch, device, cpu=(rank == 0 and a.cpu_seconds > 0))
         torch.cuda.empty_cache()
     if not a.no_extra and "serve" in extras and world == 1:
-        workloads["serve"] = measure_serve(fb, torch, device)
+        workloads["serve"] = measure_serve(fb, torch, device, n_req=a.serve_requests)
         torch.cuda.empty_cache()
 
     cpu = None
     if rank == 0 and world == 1 and a.cpu_seconds > 0:
-        v, kind, thr, desc, _ = cpu_reference(a.workload, seconds=a.cpu_seconds)
-        cpu = {"value": v, "unit": "volumes/s", "cores": thr, "kind": kind, "sample": desc}
+        cpu = cpu_baseline(a.workload, a.cpu_seconds, len(os.sched_getaffinity(0)))
+    if cpu is None and rank == 0 and world == 1 and a.cpu_seconds > 0:
+        import oracle  # the oracle port, when the reference's CPU code was not built
+        x = field(np.random.default_rng(99), (64,) + w["shape"], w["dist"], np.complex128)
+        t0, n = time.perf_counter(), 0
+        while time.perf_counter() - t0 < a.cpu_seconds:
+            y = oracle.fft3d(x)
+            if len(w["chain"]) == 2:
+                oracle.ifft3d(y)
+            n += 1
+        el = time.perf_counter() - t0
+        cpu = {"value": 64 * n / el, "unit": "volumes/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": f"oracle/fft3d_oracle.c restatement, 64 volumes per run, {n} runs"}
 
+    serve = workloads.get("serve")
+    if serve:
+        per_l["serve"] = {"batched_volumes_per_s": serve["batched_poisson"]["volumes_per_s"],
+                          "p50_s": serve["batched_poisson"]["p50_s"],
+                          "p99_s": serve["batched_poisson"]["p99_s"],
+                          "plain_fp64_p99_s": serve["plain_fp64_poisson_own_rate"]["p99_s"],
+                          "n_requests": serve["n_requests"]}
     line = {"metric": metric, "value": value, "unit": "volumes/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": a.workload, "shape": list(w["shape"]),
-                       "global_batch": world * w["batch"], "per_gpu_batch": w["batch"],
-                       "precision": "c128" if w["prec"] == 0 else "c64",
-                       "step": "forward+inverse" if len(w["chain"]) == 2 else "forward",
-                       "l2": (f"inputs larger than L2 ({wl.bytes / 2**20:.0f} MiB per buffer, "
-                              f"{wl.nsets} rotating buffer sets)"),
-                       "parallelism": f"dp{world} (volumes sharded, no collective)",
-                       "timing": dict(TIMING)},
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if w["prec"] == 0 else "f32",
+            "data": "synthetic", "config": make_config(a.workload, world),
+            "timing": dict(TIMING),
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "clocks": clocks, "gpu_launches": a.steps * wl.launches_per_step(),
-            "workloads": workloads}
+            "clocks": clocks, "gpu_launches": a.steps * launches_per_step,
+            "workloads": workloads, "per_l": per_l}
     if rank == 0:
         print(json.dumps(line))
     if dist is not None:

@@ -276,6 +276,13 @@ int fft3d_b200_server_drain(fft3d_b200_server *server, double timeout_s);
 /* Latency percentiles and throughput of everything finished so far. */
 int fft3d_b200_server_get_stats(fft3d_b200_server *server, fft3d_b200_server_stats *stats);
 
+/* Per-request latencies of the first `max` finished requests, in completion
+ * order: tickets[k] finished latency_s[k] seconds after its submission (host
+ * clock).  Returns how many were written (a negative status on bad arguments),
+ * so a caller can take percentiles over a steady-state window of the stream. */
+long long fft3d_b200_server_latencies(fft3d_b200_server *server, unsigned long long *tickets,
+                                      double *latency_s, long long max);
+
 void fft3d_b200_server_destroy(fft3d_b200_server *server);
 
 /* Run the segments as one persistent batch launch on `stream` WITHOUT allocating

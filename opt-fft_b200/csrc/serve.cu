@@ -97,6 +97,7 @@ struct fft3d_b200_server {
     int status = FFT3D_B200_OK;
     // statistics
     std::vector<double> lat;
+    std::vector<unsigned long long> lat_ticket;  // ticket of each lat entry
     long long volumes = 0, batches = 0, batched_requests = 0;
     double t_first = 0, t_last = 0;
 };
@@ -211,6 +212,7 @@ static void server_loop(fft3d_b200_server *s)
             if (q != cudaSuccess) s->status = FFT3D_B200_ERR_CUDA;
             for (const ServeReq &r : slot.reqs) {
                 s->lat.push_back(t - r.t_submit);
+                s->lat_ticket.push_back(r.ticket);
                 s->completed.push_back(r.ticket);
                 s->volumes += r.seg.batch;
                 ++s->finished;
@@ -446,6 +448,19 @@ extern "C" int fft3d_b200_server_get_stats(fft3d_b200_server *s, fft3d_b200_serv
         out->span_s = span;
     }
     return s->status;
+}
+
+extern "C" long long fft3d_b200_server_latencies(fft3d_b200_server *s, unsigned long long *tickets,
+                                                double *latency_s, long long max)
+{
+    if (!s || max < 0 || (max > 0 && (!tickets || !latency_s))) return FFT3D_B200_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(s->mu);
+    const long long n = std::min<long long>(max, (long long)s->lat.size());
+    for (long long k = 0; k < n; ++k) {
+        tickets[k] = s->lat_ticket[(size_t)k];
+        latency_s[k] = s->lat[(size_t)k];
+    }
+    return n;
 }
 
 extern "C" void fft3d_b200_server_destroy(fft3d_b200_server *s)

@@ -64,6 +64,14 @@ class Segment(ctypes.Structure):
                 ("batch", ctypes.c_longlong), ("in_", ctypes.c_void_p), ("out", ctypes.c_void_p)]
 
 
+def segment_dtype():
+    """numpy record layout of Segment (for streams of many requests)."""
+    import numpy as np
+    return np.dtype({"names": ["n0", "n1", "n2", "direction", "precision", "batch", "in_", "out"],
+                     "formats": ["i4", "i4", "i4", "i4", "i4", "i8", "u8", "u8"],
+                     "offsets": [0, 4, 8, 12, 16, 24, 32, 40], "itemsize": 48})
+
+
 class ServerStats(ctypes.Structure):
     _fields_ = [("requests", ctypes.c_longlong), ("volumes", ctypes.c_longlong),
                 ("launches", ctypes.c_longlong), ("mean_requests_per_launch", ctypes.c_double),
@@ -105,7 +113,8 @@ EXPORTS = {
                      "fft3d_b200_server_create", "fft3d_b200_server_submit",
                      "fft3d_b200_server_submit_many",
                      "fft3d_b200_server_poll", "fft3d_b200_server_drain",
-                     "fft3d_b200_server_get_stats", "fft3d_b200_server_destroy"],
+                     "fft3d_b200_server_get_stats", "fft3d_b200_server_latencies",
+                     "fft3d_b200_server_destroy"],
 }
 
 
@@ -179,6 +188,8 @@ def _load():
         "fft3d_b200_server_poll": ([vp, ctypes.POINTER(ctypes.c_ulonglong), i], i),
         "fft3d_b200_server_drain": ([vp, ctypes.c_double], i),
         "fft3d_b200_server_get_stats": ([vp, ctypes.POINTER(ServerStats)], i),
+        "fft3d_b200_server_latencies": ([vp, ctypes.POINTER(ctypes.c_ulonglong),
+                                         ctypes.POINTER(ctypes.c_double), ll], ll),
         "fft3d_b200_server_destroy": ([vp], None),
     }
     for name, (args, res) in sig.items():
@@ -492,6 +503,35 @@ class Server:
         _check(_lib.fft3d_b200_server_submit_many(self._h, arr, times, len(segs), tk),
                "server_submit_many")
         return [tk[k] for k in range(len(segs))]
+
+    def submit_array(self, segs, arrival_s=None):
+        """submit_many for a numpy array of segment_dtype() records (large
+        streams); returns the tickets as a numpy array."""
+        import numpy as np
+        segs = np.ascontiguousarray(segs, dtype=segment_dtype())
+        n = len(segs)
+        times = None
+        if arrival_s is not None:
+            arrival_s = np.ascontiguousarray(arrival_s, dtype=np.float64)
+            times = arrival_s.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        tk = np.zeros(max(1, n), dtype=np.uint64)
+        _check(_lib.fft3d_b200_server_submit_many(
+            self._h, segs.ctypes.data_as(ctypes.POINTER(Segment)), times, n,
+            tk.ctypes.data_as(ctypes.POINTER(ctypes.c_ulonglong))), "server_submit_many")
+        return tk[:n]
+
+    def latencies(self):
+        """(tickets, latency_s) of every finished request, in completion order."""
+        import numpy as np
+        n = self.stats()["requests"]
+        tk = np.zeros(max(1, n), dtype=np.uint64)
+        lat = np.zeros(max(1, n), dtype=np.float64)
+        got = _lib.fft3d_b200_server_latencies(
+            self._h, tk.ctypes.data_as(ctypes.POINTER(ctypes.c_ulonglong)),
+            lat.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n)
+        if got < 0:
+            raise Fft3dError(int(got), "server_latencies")
+        return tk[:got], lat[:got]
 
     def poll(self, max_n=4096):
         buf = (ctypes.c_ulonglong * max_n)()

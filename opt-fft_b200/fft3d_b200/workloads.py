@@ -12,9 +12,9 @@ import numpy as np
 SIDES = (6, 8, 12, 16, 17, 24, 36)
 
 
-def request_stream(n: int, rate_hz: float, seed: int = 2024):
-    """n requests: list of dicts with arrival time `t` (seconds from 0),
-    `shape`, `batch`, `direction` (-1/+1) and `precision` (0 c128, 1 c64)."""
+def request_arrays(n: int, rate_hz: float, seed: int = 2024):
+    """The stream as arrays: arrival time t (seconds from 0), side L, volume
+    count, direction (-1/+1) and precision (0 c128, 1 c64) of each request."""
     rng = np.random.default_rng(seed)
     p = np.array([1.0 / L for L in SIDES])
     p /= p.sum()
@@ -25,8 +25,35 @@ def request_stream(n: int, rate_hz: float, seed: int = 2024):
     precision = np.where(rng.random(n) < 0.75, 0, 1)
     gaps = rng.exponential(1.0 / rate_hz, n) if rate_hz > 0 else np.zeros(n)
     t = np.cumsum(gaps) - (gaps[0] if n else 0.0)
-    return [{"t": float(t[k]), "shape": (int(sides[k]),) * 3, "batch": int(counts[k]),
-             "direction": int(direction[k]), "precision": int(precision[k])} for k in range(n)]
+    return {"t": t, "side": sides.astype(np.int64), "batch": counts.astype(np.int64),
+            "direction": direction.astype(np.int64), "precision": precision.astype(np.int64)}
+
+
+def request_stream(n: int, rate_hz: float, seed: int = 2024):
+    """n requests: list of dicts with arrival time `t` (seconds from 0),
+    `shape`, `batch`, `direction` (-1/+1) and `precision` (0 c128, 1 c64)."""
+    a = request_arrays(n, rate_hz, seed)
+    return [{"t": float(a["t"][k]), "shape": (int(a["side"][k]),) * 3, "batch": int(a["batch"][k]),
+             "direction": int(a["direction"][k]), "precision": int(a["precision"][k])}
+            for k in range(n)]
+
+
+def arena_offsets(nbytes, arena_bytes):
+    """Byte offset of each request's buffer in a rotating arena: requests take
+    consecutive ranges in arrival order and wrap to the start when the next one
+    would run past the end, so a stream far larger than the arena cycles
+    through it (a request never straddles the end)."""
+    nbytes = np.asarray(nbytes, dtype=np.int64)
+    if len(nbytes) and int(nbytes.max()) > arena_bytes:
+        raise ValueError("a request is larger than the arena")
+    start = np.empty_like(nbytes)
+    pos = 0
+    for k, b in enumerate(nbytes.tolist()):
+        if pos + b > arena_bytes:
+            pos = 0
+        start[k] = pos
+        pos += b
+    return start
 
 
 def volume_bytes(req) -> int:

@@ -19,6 +19,24 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")
 
 
+# Measured errors of GPU results against the oracle, one record per checked
+# result; written as JSON lines to $FFT3D_B200_ERR_REPORT at the end of a session.
+_ERRORS = []
+
+
+def record_error(case, variant, err, tol):
+    _ERRORS.append({"case": case, "variant": variant, "rel_l2": float(err), "tol": tol})
+
+
+def pytest_sessionfinish(session, exitstatus):
+    path = os.environ.get("FFT3D_B200_ERR_REPORT")
+    if path and _ERRORS:
+        import json
+        with open(path, "w") as f:
+            for r in _ERRORS:
+                f.write(json.dumps(r) + "\n")
+
+
 def field(rng, shape, dist="uniform", dtype=np.complex128):
     """Seeded synthetic input: re/im i.i.d. uniform[-1,1) or standard normal."""
     if dist == "uniform":

@@ -22,7 +22,7 @@ import fft3d_b200 as fb  # noqa: E402
 
 KINDS = [(6, 6, 6), (8, 8, 8), (12, 12, 12), (16, 16, 16), (17, 17, 17), (24, 24, 24),
          (36, 36, 36), (8, 8, 16), (16, 16, 32)]
-C64_TOL = 2e-6
+C64_TOL = 1e-6
 C128_TOL = 1e-13
 
 # the batching configuration: (shape, volumes)

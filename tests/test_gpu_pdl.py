@@ -22,7 +22,7 @@ pytestmark = pytest.mark.gpu
 import fft3d_b200 as fb  # noqa: E402
 
 C128_TOL = 1e-13
-C64_TOL = 2e-6
+C64_TOL = 1e-6
 ROUNDS = 4
 
 GEOMS = [((8, 8, 8), fb.C128), ((17, 17, 17), fb.C128), ((24, 24, 24), fb.C128),

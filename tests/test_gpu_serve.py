@@ -21,7 +21,7 @@ import fft3d_b200 as fb  # noqa: E402
 from fft3d_b200.workloads import request_stream  # noqa: E402
 
 C128_TOL = 1e-13
-C64_TOL = 2e-6
+C64_TOL = 1e-6
 
 
 def materialise(reqs, seed=1):

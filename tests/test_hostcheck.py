@@ -16,7 +16,7 @@ import oracle
 from conftest import GOLDEN, field
 
 C128_TOL = 1e-13
-C64_TOL = 2e-6
+C64_TOL = 1e-6
 
 # (shape, alg, vpc) pairs the emulator was built with
 GEOMS = [((6, 6, 6), 0, 16), ((8, 8, 8), 0, 8), ((12, 12, 12), 0, 2), ((16, 16, 16), 0, 1),

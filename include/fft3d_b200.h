@@ -36,6 +36,7 @@ extern "C" {
 #define FFT3D_B200_ERR_BUDGET (-7)      /* request larger than the admission budget */
 #define FFT3D_B200_ERR_OVERLAP (-8)     /* in and out overlap; transforms are out-of-place */
 #define FFT3D_B200_ERR_BUSY (-9)        /* server queue full; retry later */
+#define FFT3D_B200_ERR_PEER (-10)       /* multi-GPU: two listed devices cannot reach each other */
 
 #define FFT3D_B200_FORWARD (-1)  /* exp(-2*pi*i k.j/n), unnormalised */
 #define FFT3D_B200_BACKWARD (+1) /* exp(+2*pi*i k.j/n), scaled by 1/(n0*n1*n2) */

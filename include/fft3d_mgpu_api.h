@@ -41,7 +41,11 @@ int fft3d_mgpu_supports(int L, int ngpus);
 
 /* bench/mgpu/fft3d_mgpu_api.h:81-83: all setup (buffers, streams, events, peer
  * access, tables).  `devices` lists the CUDA ordinals, length ngpus.  NULL if
- * unsupported or if a device, an allocation or peer access fails. */
+ * unsupported or if a device, an allocation or peer access fails; the reason is
+ * then fft3d_b200_last_status() (fft3d_b200.h): FFT3D_B200_ERR_PEER when two
+ * distinct listed devices cannot access each other's memory (checked for every
+ * pair before anything is allocated), FFT3D_B200_ERR_INVALID for an ordinal
+ * that is not a visible device. */
 fft3d_mgpu_plan *fft3d_mgpu_create(int L, int batch, int ngpus, const int *devices);
 
 /* Extension, no counterpart in the reference: `inverse` nonzero builds the

@@ -15,6 +15,8 @@ namespace fft3d {
 
 void ensure_host_tables();
 int ensure_device_tables(int device);
+// Set the calling thread's fft3d_b200_last_status() and return the code.
+int record_status(int s);
 
 // Kernel family of a registry entry.
 enum Family : int {

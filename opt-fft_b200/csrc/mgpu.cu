@@ -329,14 +329,41 @@ extern "C" void fft3d_mgpu_destroy(fft3d_mgpu_plan *p)
 extern "C" fft3d_mgpu_plan *fft3d_mgpu_create_ex(int L, int batch, int ngpus, const int *devices,
                                                  int inverse)
 {
-    if (!fft3d_mgpu_supports(L, ngpus) || batch < 1 || !devices) return nullptr;
+    if (!devices || batch < 1) {
+        record_status(FFT3D_B200_ERR_INVALID);
+        return nullptr;
+    }
+    if (!fft3d_mgpu_supports(L, ngpus)) {
+        record_status(FFT3D_B200_ERR_UNSUPPORTED);
+        return nullptr;
+    }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess) {
         cudaGetLastError();
+        record_status(FFT3D_B200_ERR_CUDA);
         return nullptr;
     }
     for (int g = 0; g < ngpus; ++g)
-        if (devices[g] < 0 || devices[g] >= ndev) return nullptr;
+        if (devices[g] < 0 || devices[g] >= ndev) {
+            record_status(FFT3D_B200_ERR_INVALID);
+            return nullptr;
+        }
+    // every pair of distinct listed devices must reach each other's memory:
+    // the exchange is peer stores from inside the compute kernels
+    for (int g = 0; g < ngpus; ++g)
+        for (int h = 0; h < ngpus; ++h) {
+            if (devices[h] == devices[g]) continue;
+            int can = 0;
+            if (cudaDeviceCanAccessPeer(&can, devices[g], devices[h]) != cudaSuccess) {
+                cudaGetLastError();
+                record_status(FFT3D_B200_ERR_CUDA);
+                return nullptr;
+            }
+            if (!can) {
+                record_status(FFT3D_B200_ERR_PEER);
+                return nullptr;
+            }
+        }
     int prev = -1;
     cudaGetDevice(&prev);
     fft3d_mgpu_plan *p = new fft3d_mgpu_plan();
@@ -398,8 +425,10 @@ extern "C" fft3d_mgpu_plan *fft3d_mgpu_create_ex(int L, int batch, int ngpus, co
     if (!ok) {
         cudaGetLastError();
         fft3d_mgpu_destroy(p);
+        record_status(FFT3D_B200_ERR_CUDA);
         return nullptr;
     }
+    record_status(FFT3D_B200_OK);
     return p;
 }
 

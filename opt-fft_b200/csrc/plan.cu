@@ -35,6 +35,8 @@ static int set_status(int s)
     return s;
 }
 
+int record_status(int s) { return set_status(s); }
+
 int element_bytes(int precision) { return precision == FFT3D_B200_C64 ? 8 : 16; }
 
 const std::vector<KernelEntry> &registry()
@@ -946,6 +948,7 @@ extern "C" const char *fft3d_b200_status_string(int s)
     case FFT3D_B200_ERR_BUDGET: return "request exceeds the admission budget";
     case FFT3D_B200_ERR_OVERLAP: return "input and output overlap";
     case FFT3D_B200_ERR_BUSY: return "queue full";
+    case FFT3D_B200_ERR_PEER: return "listed devices cannot access each other's memory";
     default: return "unknown status";
     }
 }

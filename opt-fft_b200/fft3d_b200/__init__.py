@@ -32,6 +32,7 @@ ERR_TIMEOUT = -6
 ERR_BUDGET = -7
 ERR_OVERLAP = -8
 ERR_BUSY = -9
+ERR_PEER = -10
 
 FORWARD = -1
 BACKWARD = +1

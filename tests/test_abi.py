@@ -61,7 +61,7 @@ def test_names_and_supports():
 
 def test_status_strings():
     lib = fb.lib()
-    for s in range(0, -10, -1):
+    for s in range(0, -11, -1):
         assert lib.fft3d_b200_status_string(s)
     assert lib.fft3d_b200_status_string(-1234) == b"unknown status"
 

@@ -94,3 +94,28 @@ def test_mgpu_create_refuses_bad_arguments():
     assert not lib.fft3d_mgpu_create(64, 1, 2, devs)         # no such device
     assert not lib.fft3d_mgpu_create(100, 1, 2, (ctypes.c_int * 2)(0, 0))  # unsupported L
     assert not lib.fft3d_mgpu_create(64, 0, 1, (ctypes.c_int * 1)(0))     # empty batch
+
+
+@pytest.mark.gpu
+def test_mgpu_create_refuses_devices_it_cannot_use():
+    """A listed ordinal that is not a visible device, or (with two or more GPUs
+    visible) a pair without peer access, gives NULL and a status -- before any
+    allocation.  With one GPU visible only the first case can be shown here; the
+    device-repeat tests above never cross NVLink."""
+    import torch
+    lib = fb.lib()
+    n = torch.cuda.device_count()
+    devs = (ctypes.c_int * 2)(0, n)  # ordinal n does not exist
+    assert lib.fft3d_mgpu_create(64, 1, 2, devs) is None
+    assert lib.fft3d_b200_last_status() == fb.ERR_INVALID
+    devs = (ctypes.c_int * 3)(0, 0, 0)  # 64 is not split over 3
+    assert lib.fft3d_mgpu_create(64, 1, 3, devs) is None
+    assert lib.fft3d_b200_last_status() == fb.ERR_UNSUPPORTED
+    if n >= 2:
+        devs = (ctypes.c_int * 2)(0, 1)
+        h = lib.fft3d_mgpu_create(64, 1, 2, devs)
+        if h is None:
+            assert lib.fft3d_b200_last_status() == fb.ERR_PEER
+        else:
+            assert lib.fft3d_b200_last_status() == fb.OK
+            lib.fft3d_mgpu_destroy(h)

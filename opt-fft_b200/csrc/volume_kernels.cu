@@ -93,6 +93,41 @@ void register_kernels(std::vector<KernelEntry> &out)
     FFT3D_VOL(16, 16, 32, float, 0, 1, 512, 1);
     FFT3D_VOL(13, 13, 13, float, 0, 4, 704, 1);
     FFT3D_VOL(23, 23, 23, float, 0, 1, 544, 1);
+
+    // The other extents of the reference's oracle and tests
+    // (python/test_fft3d.py:25-36): small cubes, 10^3, 15^3 and anisotropic
+    // volumes, degenerate axes of length 1 included.  One CTA per group of
+    // volumes; about 256-700 threads and 25-55 KB of shared memory a CTA.
+    FFT3D_VOL(1, 1, 1, double, 0, 64, 64, 1);
+    FFT3D_VOL(3, 3, 3, double, 0, 32, 288, 1);
+    FFT3D_VOL(4, 4, 4, double, 0, 16, 256, 1);
+    FFT3D_VOL(9, 9, 9, double, 0, 4, 352, 1);
+    FFT3D_VOL(10, 10, 10, double, 0, 2, 224, 1);
+    FFT3D_VOL(15, 15, 15, double, 0, 1, 256, 1);
+    FFT3D_VOL(2, 3, 5, double, 0, 32, 320, 1);
+    FFT3D_VOL(7, 11, 13, double, 0, 2, 288, 1);
+    FFT3D_VOL(5, 8, 12, double, 0, 4, 384, 1);
+    FFT3D_VOL(13, 5, 8, double, 0, 4, 416, 1);
+    FFT3D_VOL(17, 2, 2, double, 0, 16, 544, 1);
+    FFT3D_VOL(32, 8, 4, double, 0, 2, 256, 1);
+    FFT3D_VOL(1, 8, 8, double, 0, 32, 256, 1);
+    FFT3D_VOL(8, 1, 8, double, 0, 32, 256, 1);
+    FFT3D_VOL(8, 8, 1, double, 0, 32, 256, 1);
+    FFT3D_VOL(1, 1, 1, float, 0, 128, 128, 1);
+    FFT3D_VOL(3, 3, 3, float, 0, 64, 576, 1);
+    FFT3D_VOL(4, 4, 4, float, 0, 32, 512, 1);
+    FFT3D_VOL(9, 9, 9, float, 0, 8, 672, 1);
+    FFT3D_VOL(10, 10, 10, float, 0, 4, 416, 1);
+    FFT3D_VOL(15, 15, 15, float, 0, 2, 480, 1);
+    FFT3D_VOL(2, 3, 5, float, 0, 64, 512, 1);
+    FFT3D_VOL(7, 11, 13, float, 0, 4, 576, 1);
+    FFT3D_VOL(5, 8, 12, float, 0, 8, 768, 1);
+    FFT3D_VOL(13, 5, 8, float, 0, 8, 832, 1);
+    FFT3D_VOL(17, 2, 2, float, 0, 32, 1024, 1);
+    FFT3D_VOL(32, 8, 4, float, 0, 4, 512, 1);
+    FFT3D_VOL(1, 8, 8, float, 0, 64, 512, 1);
+    FFT3D_VOL(8, 1, 8, float, 0, 64, 512, 1);
+    FFT3D_VOL(8, 8, 1, float, 0, 64, 512, 1);
 }
 
 }  // namespace fft3d

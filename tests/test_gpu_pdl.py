@@ -73,7 +73,9 @@ def test_dependent_launches_every_variant(shape, prec):
         inv.check()
         ey = oracle.rel_error_per_volume(y.cpu().numpy(), want_y).max()
         ex = oracle.rel_error_per_volume(x.cpu().numpy(), x0.astype(np.complex128)).max()
-        assert ey < ROUNDS * t, f"{v}: forward after {ROUNDS} round trips, rel err {ey:.3e}"
+        # y has been through 2R-1 transforms and x through 2R: per-transform
+        # errors add at most linearly along the chain
+        assert ey < (2 * ROUNDS - 1) * t, f"{v}: forward after {ROUNDS} round trips, rel err {ey:.3e}"
         assert ex < 2 * ROUNDS * t, f"{v}: round trips, rel err {ex:.3e}"
         fwd.close()
         inv.close()

@@ -431,6 +431,17 @@ static const EmuEntry kEmu[] = {
     EMU_TPRQ(36, 36, 36, 2), EMU_TPRP(45, 45, 45, 3), EMU_TPRP(6, 9, 5, 3), EMU_TPRQ(6, 9, 5, 3), EMU_TPRQF(3), EMU_TPRQF(2), EMU_TPRQF(4), EMU_TPST(LineCT64, 64, double), EMU_TPST(LineCT64, 64, float), EMU_TPST(LinePFA45, 45, double),
     EMU_TPST(LinePFA36, 36, double), EMU_TPST(LinePFA36, 36, float),
     EMU_TPR(6, 9, 5, 3),
+    // the group sizes the VOLUME kernels of these extents use
+    EMU(1, 1, 1, double, 0, 64),  EMU(3, 3, 3, double, 0, 32),   EMU(4, 4, 4, double, 0, 16),
+    EMU(9, 9, 9, double, 0, 4),   EMU(10, 10, 10, double, 0, 2), EMU(15, 15, 15, double, 0, 1),
+    EMU(2, 3, 5, double, 0, 32),  EMU(5, 8, 12, double, 0, 4),   EMU(13, 5, 8, double, 0, 4),
+    EMU(17, 2, 2, double, 0, 16), EMU(32, 8, 4, double, 0, 2),   EMU(1, 8, 8, double, 0, 32),
+    EMU(8, 1, 8, double, 0, 32),  EMU(8, 8, 1, double, 0, 32),
+    EMU(1, 1, 1, float, 0, 128),  EMU(3, 3, 3, float, 0, 64),    EMU(4, 4, 4, float, 0, 32),
+    EMU(9, 9, 9, float, 0, 8),    EMU(10, 10, 10, float, 0, 4),  EMU(15, 15, 15, float, 0, 2),
+    EMU(2, 3, 5, float, 0, 64),   EMU(7, 11, 13, float, 0, 4),   EMU(5, 8, 12, float, 0, 8),
+    EMU(13, 5, 8, float, 0, 8),   EMU(17, 2, 2, float, 0, 32),   EMU(32, 8, 4, float, 0, 4),
+    EMU(1, 8, 8, float, 0, 64),   EMU(8, 1, 8, float, 0, 64),    EMU(8, 8, 1, float, 0, 64),
 };
 
 // The chain kernel's per-CTA loop (chain_kernels.cu k_chain) for one volume per CTA.

@@ -31,7 +31,11 @@ C64_TOL = 1e-6
 
 GEOMS = [(6, 6, 6), (8, 8, 8), (12, 12, 12), (16, 16, 16), (17, 17, 17), (24, 24, 24),
          (8, 8, 16), (16, 16, 32), (36, 36, 36), (13, 13, 13), (23, 23, 23), (45, 45, 45),
-         (64, 64, 64)]
+         (64, 64, 64),
+         # the other extents of the reference's tests (python/test_fft3d.py:25-36)
+         (1, 1, 1), (3, 3, 3), (4, 4, 4), (9, 9, 9), (10, 10, 10), (15, 15, 15), (2, 3, 5),
+         (7, 11, 13), (5, 8, 12), (13, 5, 8), (17, 2, 2), (32, 8, 4), (1, 8, 8), (8, 1, 8),
+         (8, 8, 1)]
 TDT = {fb.C128: torch.complex128, fb.C64: torch.complex64}
 NDT = {fb.C128: np.complex128, fb.C64: np.complex64}
 
@@ -80,6 +84,10 @@ def test_every_variant_matches_oracle(shape, prec, direction):
             # persistent kernels: every CTA walks >= 2 groups and one group is partial
             vpc = int(v.split(" vpc")[1].split()[0])
             b = 2 * 148 * vpc + vpc // 2 + 1
+        elif v.startswith("volume"):
+            # several CTAs and a partial group
+            vpc = int(v.split(" vpc")[1].split()[0])
+            b = max(b, 2 * vpc + vpc // 2 + 1)
         elif v.startswith("twopass"):
             # beyond the scratch ring (about 40 volumes at a full grid): slots are reused
             b = 100

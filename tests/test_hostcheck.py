@@ -25,10 +25,19 @@ GEOMS = [((6, 6, 6), 0, 16), ((8, 8, 8), 0, 8), ((12, 12, 12), 0, 2), ((16, 16, 
          ((9, 9, 9), 0, 2), ((5, 8, 12), 0, 1), ((32, 8, 4), 0, 1), ((13, 5, 8), 0, 1),
          ((4, 4, 4), 0, 2), ((1, 8, 8), 0, 1), ((8, 1, 8), 0, 1), ((8, 8, 1), 0, 1),
          ((1, 1, 1), 0, 1), ((3, 3, 3), 0, 1), ((17, 2, 2), 0, 1), ((13, 13, 13), 0, 2),
-         ((23, 23, 23), 0, 1)]
+         ((23, 23, 23), 0, 1),
+         # the group sizes of the VOLUME kernels for the reference's other extents
+         ((1, 1, 1), 0, 64), ((3, 3, 3), 0, 32), ((4, 4, 4), 0, 16), ((9, 9, 9), 0, 4),
+         ((10, 10, 10), 0, 2), ((15, 15, 15), 0, 1), ((2, 3, 5), 0, 32), ((5, 8, 12), 0, 4),
+         ((13, 5, 8), 0, 4), ((17, 2, 2), 0, 16), ((32, 8, 4), 0, 2), ((1, 8, 8), 0, 32),
+         ((8, 1, 8), 0, 32), ((8, 8, 1), 0, 32)]
 GEOMS64 = [((6, 6, 6), 0, 32), ((8, 8, 8), 0, 16), ((12, 12, 12), 0, 4), ((16, 16, 16), 0, 2),
            ((17, 17, 17), 0, 2), ((17, 17, 17), 1, 2), ((24, 24, 24), 0, 1), ((8, 8, 16), 0, 16),
-           ((16, 16, 32), 0, 1), ((36, 36, 36), 0, 1), ((13, 13, 13), 0, 4), ((23, 23, 23), 0, 1)]
+           ((16, 16, 32), 0, 1), ((36, 36, 36), 0, 1), ((13, 13, 13), 0, 4), ((23, 23, 23), 0, 1),
+           ((1, 1, 1), 0, 128), ((3, 3, 3), 0, 64), ((4, 4, 4), 0, 32), ((9, 9, 9), 0, 8),
+           ((10, 10, 10), 0, 4), ((15, 15, 15), 0, 2), ((2, 3, 5), 0, 64), ((7, 11, 13), 0, 4),
+           ((5, 8, 12), 0, 8), ((13, 5, 8), 0, 8), ((17, 2, 2), 0, 32), ((32, 8, 4), 0, 4),
+           ((1, 8, 8), 0, 64), ((8, 1, 8), 0, 64), ((8, 8, 1), 0, 64)]
 
 
 def run(hc, x, shape, prec, sign, alg, vpc):

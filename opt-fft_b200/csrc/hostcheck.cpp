@@ -231,6 +231,72 @@ static void emulate_twopass_regs(const void *vin, void *vout, long long nvol)
     }
 }
 
+// The lane-split TWOPASS kernel (k_twopass_lanes): rows at the odd pitch N|1,
+// every line's P lanes run by lane_split_line_host with the kernel's own index
+// maps -- z pass in place, y pass into the slot, x pass to the output.
+// Tickets, ring and dependency checks as emulate_twopass.
+template <int N, int S, int G, int P>
+static void emulate_twopass_lanes(const void *vin, void *vout, long long nvol)
+{
+    using T = double;
+    constexpr int PITCH = N | 1;
+    using TG = TwoPassGeom<N, N, N, T, G, PITCH>;
+    using XG = typename TG::XG;
+    using YG = typename TG::YG;
+    constexpr int LINES = G * N;
+    const T scale = S > 0 ? T(1) / T(TG::V) : T(1);
+    int lag = 0;
+    const int R = twopass_ring_size(TG::NA, TG::NB, 7, &lag);
+    std::vector<cx<T>> sm((size_t)TG::PV), ring((size_t)R * TG::V, cx<T>{T(-777.0), T(555.0)});
+    const cx<T> *in = (const cx<T> *)vin;
+    cx<T> *out = (cx<T> *)vout;
+    const long long total = (long long)(TG::NA + TG::NB) * nvol;
+    std::vector<long long> cnt_plane(R, 0), cnt_row(R, 0);
+    for (long long tk = 0; tk < total; ++tk) {
+        const TwoPassItem it = twopass_decode(tk, nvol, TG::NA, TG::NB, lag);
+        const int slot = (int)(it.vol % R);
+        const long long round = it.vol / R;
+        cx<T> *sv = ring.data() + slot * TG::V;
+        if (it.plane ? cnt_row[slot] < TG::NB * round : cnt_plane[slot] < TG::NA * (round + 1))
+            g_twopass_violations++;
+        (it.plane ? cnt_plane : cnt_row)[slot]++;
+        for (auto &e : sm) e = {T(12345.0), T(-6789.0)};
+        if (it.plane) {
+            const cx<T> *rows = in + it.vol * TG::V + (long long)it.j * G * N * N;
+            for (int r = 0; r < XG::ROWS; ++r)
+                for (int z = 0; z < N; ++z) sm[XG::off(r, z)] = rows[(long long)r * N + z];
+            for (int r = 0; r < LINES; ++r) {
+                cx<T> *row = sm.data() + XG::off(r, 0);
+                lane_split_line_host<N, P, S, T>([&](int z) { return row[z]; },
+                                                 [&](int z, cx<T> v) { row[z] = v; });
+            }
+            for (int l = 0; l < LINES; ++l) {
+                const int g = l / N, z = l % N;
+                const cx<T> *col = sm.data() + XG::off(g * N, z);
+                cx<T> *o = sv + (long long)(it.j * G + g) * N * N + z;
+                lane_split_line_host<N, P, S, T>([&](int y) { return col[y * PITCH]; },
+                                                 [&](int y, cx<T> v) { o[y * N] = v; });
+            }
+        } else {
+            for (int q = 0; q < N * G; ++q) {
+                const int x = q / G, yl = q % G;
+                for (int z = 0; z < N; ++z) sm[YG::off(q, z)] = sv[((long long)x * N + it.j * G + yl) * N + z];
+            }
+            cx<T> *gvol = out + it.vol * TG::V;
+            for (int l = 0; l < LINES; ++l) {
+                const int yl = l / N, z = l % N;
+                const cx<T> *col = sm.data() + YG::off(yl, z);
+                cx<T> *o = gvol + (long long)(it.j * G + yl) * N + z;
+                lane_split_line_host<N, P, S, T>([&](int x) { return col[x * G * PITCH]; },
+                                                 [&](int x, cx<T> v) {
+                                                     if (S > 0) v = cscale(v, scale);
+                                                     o[(long long)x * N * N] = v;
+                                                 });
+            }
+        }
+    }
+}
+
 // The staged TWOPASS kernel (k_twopass_staged; staged.cuh line policies):
 // rows at the kernel's pitch, z pass in place (rows end in Line::slot order),
 // y pass stored into the slot at the natural z, x pass streamed out; every
@@ -378,6 +444,9 @@ typedef void (*emu_fn)(const void *, void *, long long);
 #define EMU_TPRQF(G)                                                                          \
     {36, 36, 36, 1, -1, 540 + G, 1, &emulate_twopass_regs<36, 36, 36, float, -1, G, true, true, 38>},  \
     {36, 36, 36, 1, +1, 540 + G, 1, &emulate_twopass_regs<36, 36, 36, float, +1, G, true, true, 38>}
+#define EMU_TPL(N, G, P)                                                                      \
+    {N, N, N, 0, -1, 1024 + P, G, &emulate_twopass_lanes<N, -1, G, P>},                        \
+    {N, N, N, 0, +1, 1024 + P, G, &emulate_twopass_lanes<N, +1, G, P>}
 #define EMU_TPST(LINE, N, T)                                                                  \
     {N, N, N, sizeof(T) == 8 ? 0 : 1, -1, 701, 1, &emulate_twopass_staged<LINE, -1, T>},         \
     {N, N, N, sizeof(T) == 8 ? 0 : 1, +1, 701, 1, &emulate_twopass_staged<LINE, +1, T>}
@@ -431,6 +500,7 @@ static const EmuEntry kEmu[] = {
     EMU_TPRQ(36, 36, 36, 2), EMU_TPRP(45, 45, 45, 3), EMU_TPRP(6, 9, 5, 3), EMU_TPRQ(6, 9, 5, 3), EMU_TPRQF(3), EMU_TPRQF(2), EMU_TPRQF(4), EMU_TPST(LineCT64, 64, double), EMU_TPST(LineCT64, 64, float), EMU_TPST(LinePFA45, 45, double),
     EMU_TPST(LinePFA36, 36, double), EMU_TPST(LinePFA36, 36, float),
     EMU_TPR(6, 9, 5, 3),
+    EMU_TPL(36, 2, 2), EMU_TPL(36, 2, 4), EMU_TPL(36, 1, 4), EMU_TPL(36, 3, 4),
     // the group sizes the VOLUME kernels of these extents use
     EMU(1, 1, 1, double, 0, 64),  EMU(3, 3, 3, double, 0, 32),   EMU(4, 4, 4, double, 0, 16),
     EMU(9, 9, 9, double, 0, 4),   EMU(10, 10, 10, double, 0, 2), EMU(15, 15, 15, double, 0, 1),

@@ -128,6 +128,87 @@ __device__ __forceinline__ void split_line(int t, bool valid, Ld ld, St st)
 }
 #endif
 
+// ---------------------------------------------------------------- explicit P, strided lanes
+//
+// The same split with P chosen by the kernel, and the P lanes of a line LS
+// apart in the warp (lane t of a line is warp lane w + t*LS, w < LS): a warp
+// holds LS lines side by side, so the 8 lanes of every shared-memory phase work
+// on 8 different lines at the same position -- with an odd row pitch no bank
+// conflicts on rows or columns -- and a global store of a warp covers LS
+// consecutive points.  36 = 2 x 18 is a Cooley-Tukey split (the 18-point DFT
+// of lane t's points x[t + 2 n2], then W_36^(t k2), then one exchange);
+// 36 = 4 x 9 is the Good-Thomas split above.
+template <int N, int P>
+struct LaneSplit {
+    static constexpr int Q = N / P;
+    static_assert(P * Q == N && (P & (P - 1)) == 0, "P a power of two dividing N");
+    static constexpr bool PFA = ce_gcd(P, Q) == 1;
+    static constexpr int A = PFA ? Q * ce_modinv(Q % P, P) : 0;
+    static constexpr int B = PFA ? P * ce_modinv(P % Q, Q) : 0;
+    FFT_HD static constexpr int in(int t, int n2) { return PFA ? (Q * t + P * n2) % N : t + P * n2; }
+    FFT_HD static constexpr int out(int k1, int k2) { return PFA ? (A * k1 + B * k2) % N : k2 + Q * k1; }
+};
+
+// W_N^(t k2) of a Cooley-Tukey split (k2 a constant after unrolling).  With
+// P = 2 the twiddle of lane 1 is a constant-bank operand and lane 0 selects 1.
+template <int N, int P, int S, typename T>
+FFT_HD cx<T> lane_twiddle(cx<T> a, int t, int k2)
+{
+    if (k2 == 0) return a;
+    if constexpr (P == 2) {
+        const auto w = Tab<T>::tw(tw_off(N) + k2);
+        const T c = t ? w.x : T(1);
+        const T s = t ? ((S > 0) ? w.y : -w.y) : T(0);
+        return {a.re * c - a.im * s, a.re * s + a.im * c};
+    } else {
+        return ctwiddle<N, S, T>(a, t * k2);
+    }
+}
+
+#if defined(__CUDACC__)
+// One radix-2 stage of the P-point DFT across the lanes (distance H*LS).
+template <int H, int LS, int S, typename T>
+__device__ __forceinline__ void xlane_stage_strided(cx<T> &a, int t)
+{
+    if constexpr (H >= 1) {
+        cx<T> b;
+        b.re = __shfl_xor_sync(0xffffffffu, a.re, H * LS);
+        b.im = __shfl_xor_sync(0xffffffffu, a.im, H * LS);
+        const bool hi = (t & H) != 0;
+        const T sg = hi ? T(-1) : T(1);  // low lane a + b, high lane b - a
+        a = {fma(sg, a.re, b.re), fma(sg, a.im, b.im)};
+        if constexpr (H > 1) {
+            if (hi) a = ctwiddle<2 * H, S, T>(a, t & (H - 1));
+        }
+        xlane_stage_strided<H / 2, LS, S, T>(a, t);
+    }
+}
+
+// Lane t (0 <= t < P) of a line whose lanes are LS apart: load Q points, transform,
+// store Q outputs.  Lanes with valid == false exchange zeros and store nothing;
+// the P lanes of a line are valid together.
+template <int N, int P, int LS, int S, typename T, class Ld, class St>
+__device__ __forceinline__ void lane_split_line(int t, bool valid, Ld ld, St st)
+{
+    using M = LaneSplit<N, P>;
+    cx<T> v[M::Q];
+#pragma unroll
+    for (int n2 = 0; n2 < M::Q; ++n2) v[n2] = valid ? ld(M::in(t, n2)) : cx<T>{T(0), T(0)};
+    dft<M::Q, S, T>(v);
+    if constexpr (!M::PFA) {
+#pragma unroll
+        for (int k2 = 1; k2 < M::Q; ++k2) v[k2] = lane_twiddle<N, P, S, T>(v[k2], t, k2);
+    }
+#pragma unroll
+    for (int k2 = 0; k2 < M::Q; ++k2) xlane_stage_strided<P / 2, LS, S, T>(v[k2], t);
+    const int k1 = lane_bitrev<P>(t);
+    if (valid) {
+#pragma unroll
+        for (int k2 = 0; k2 < M::Q; ++k2) st(M::out(k1, k2), v[k2]);
+    }
+}
+#endif
+
 // The lane network of xlane_stage on an array a[t] of the P lanes.
 template <int H, int P, int S, typename T>
 void xlane_stage_host(cx<T> *a)
@@ -168,6 +249,28 @@ void split_line_host(Ld ld, St st)
     }
     for (int t = 0; t < SP::P; ++t)
         for (int k2 = 0; k2 < SP::Q; ++k2) st(M::out(lane_bitrev<SP::P>(t), k2), v[t][k2]);
+}
+
+// lane_split_line for all P lanes of one line on the host (hostcheck).
+template <int N, int P, int S, typename T, class Ld, class St>
+void lane_split_line_host(Ld ld, St st)
+{
+    using M = LaneSplit<N, P>;
+    cx<T> v[P][M::Q];
+    for (int t = 0; t < P; ++t) {
+        for (int n2 = 0; n2 < M::Q; ++n2) v[t][n2] = ld(M::in(t, n2));
+        dft<M::Q, S, T>(v[t]);
+        if (!M::PFA)
+            for (int k2 = 1; k2 < M::Q; ++k2) v[t][k2] = lane_twiddle<N, P, S, T>(v[t][k2], t, k2);
+    }
+    for (int k2 = 0; k2 < M::Q; ++k2) {
+        cx<T> a[P];
+        for (int t = 0; t < P; ++t) a[t] = v[t][k2];
+        xlane_stage_host<P / 2, P, S, T>(a);
+        for (int t = 0; t < P; ++t) v[t][k2] = a[t];
+    }
+    for (int t = 0; t < P; ++t)
+        for (int k2 = 0; k2 < M::Q; ++k2) st(M::out(lane_bitrev<P>(t), k2), v[t][k2]);
 }
 
 }  // namespace fft3d

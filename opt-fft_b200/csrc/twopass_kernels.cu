@@ -639,6 +639,172 @@ __global__ void __launch_bounds__(NT, MINB)
     }
 }
 
+// TWOPASS for N^3 complex double with every line split over P lanes of a warp
+// (splitline.cuh lane_split_line: 36 = 2 x 18 Cooley-Tukey or 4 x 9 Good-Thomas),
+// under the lean item control, bulk row copies and L2 policies of
+// k_twopass_regs ("bulkqh").  A warp holds 32/P lines side by side (lane t of a
+// line is LS = 32/P lanes from lane t-1), so a lane keeps N/P points -- 18 or 9
+// complex doubles instead of 36 -- and many more warps fit an SM; the price is
+// the cross-lane exchange (P = 2: one shuffle stage, P = 4: two).  Rows sit at
+// the odd pitch N|1: every 8-lane shared-memory phase touches 8 lines at one
+// position, conflict-free along rows and columns.  The z pass works in place
+// in shared memory, the y pass stores into the scratch slot from registers,
+// the x pass streams the output.  "lanesP" in the name.
+template <int N, int S, int G, int NT, int MINB, int P>
+__global__ void __launch_bounds__(NT, MINB)
+    k_twopass_lanes(const cx<double> *__restrict__ in, cx<double> *__restrict__ out, long long nvol,
+                    double scale, int *err, unsigned char *work, int R, int D)
+{
+    pdl_begin();
+    using T = double;
+    constexpr int PITCH = N | 1;
+    using TG = TwoPassGeom<N, N, N, T, G, PITCH>;
+    using XG = typename TG::XG;
+    using YG = typename TG::YG;
+    constexpr int LS = 32 / P;                  // lines per warp, lane distance within a line
+    constexpr int WARPS = NT / 32;
+    constexpr int LINES = G * N;                // lines of one pass of an item
+    static_assert(NT % 32 == 0 && 32 % P == 0, "whole warps, P | 32");
+    constexpr uint32_t ROW_BYTES = (uint32_t)(N * sizeof(cx<T>));
+    static_assert(ROW_BYTES % 16 == 0, "bulk row copies: 16-byte rows");
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);
+    __shared__ long long s_t;
+    __shared__ int s_stop;
+    __shared__ __align__(8) uint64_t s_bar;
+    TwoPassCtl *ctl = reinterpret_cast<TwoPassCtl *>(work);
+    cx<T> *ring = reinterpret_cast<cx<T> *>(work + TWOPASS_CTL_BYTES);
+    const int tid = threadIdx.x;
+    const int warp = tid / 32, lane = tid % 32;
+    const int t = lane / LS, lw = lane % LS;   // lane of its line, line slot in the warp
+    const long long total = (long long)(TG::NA + TG::NB) * nvol;
+    uint32_t phase = 0;
+    bool copies_pending = false;
+    long long next = 0;
+    const uint64_t pol_first = l2_policy_evict_first();
+    const uint64_t pol_last = l2_policy_evict_last();
+    if (tid == 0) {
+        mbar_init(&s_bar, 1);
+        fence_mbar_init();
+        next = (long long)atomicAdd(&ctl->ticket, 1ull);
+    }
+    auto wait_copies = [&]() {
+        copies_pending = true;
+        const bool ok = mbar_wait_bounded(&s_bar, phase);
+        phase ^= 1u;
+        if (ok) copies_pending = false;
+        return ok;
+    };
+
+    for (;;) {
+        if (tid == 0) {
+            const long long tk = next;
+            int stop = tk >= total ? 1 : 0;
+            if (!stop) {
+                next = (long long)atomicAdd(&ctl->ticket, 1ull);
+                const TwoPassItem it = twopass_decode(tk, nvol, TG::NA, TG::NB, D);
+                const unsigned target = (unsigned)TG::NA * (unsigned)(it.vol / R + 1);
+                if (!it.plane && !wait_counter_geq(&ctl->cnt[it.vol % R], target, &ctl->abort)) stop = 2;
+            }
+            s_t = tk;
+            s_stop = stop;
+        }
+        __syncthreads();
+        if (s_stop) break;
+        const TwoPassItem it = twopass_decode(s_t, nvol, TG::NA, TG::NB, D);
+        const int slot = (int)(it.vol % R);
+        cx<T> *sv = ring + (long long)slot * TG::V;
+
+        if (it.plane) {
+            // 1. G contiguous planes of the input, one bulk copy per row
+            if (tid == 0) mbar_arrive_expect_tx(&s_bar, (uint32_t)XG::ROWS * ROW_BYTES);
+            const cx<T> *rows = in + it.vol * TG::V + (long long)it.j * G * N * N;
+            for (int r = tid; r < XG::ROWS; r += NT)
+                bulk_g2s_hint(sm + XG::off(r, 0), rows + (long long)r * N, ROW_BYTES, &s_bar, pol_first);
+            if (tid == 0) {
+                const unsigned target = (unsigned)TG::NB * (unsigned)(it.vol / R);
+                if (target > 0 && !wait_counter_geq(&ctl->cnt[TWOPASS_RMAX + slot], target, &ctl->abort))
+                    s_stop = 2;
+            }
+            if (!wait_copies()) s_stop = 2;
+            __syncthreads();
+            if (s_stop) break;
+            // 2. z pass in place: line = row r
+            for (int base = 0; base < LINES; base += WARPS * LS) {
+                const int r = base + warp * LS + lw;
+                const bool valid = r < LINES;
+                cx<T> *row = sm + XG::off(valid ? r : 0, 0);
+                lane_split_line<N, P, LS, S, T>(t, valid, [&](int z) { return row[z]; },
+                                                 [&](int z, cx<T> v) { row[z] = v; });
+            }
+            __syncthreads();
+            // 3. y pass into the scratch slot: line = (g, z)
+            for (int base = 0; base < LINES; base += WARPS * LS) {
+                const int l = base + warp * LS + lw;
+                const bool valid = l < LINES;
+                const int g = valid ? l / N : 0, z = l % N;
+                const cx<T> *col = sm + XG::off(g * N, z);
+                cx<T> *o = sv + (long long)(it.j * G + g) * N * N + z;
+                lane_split_line<N, P, LS, S, T>(
+                    t, valid, [&](int y) { return col[y * PITCH]; },
+                    [&](int y, cx<T> v) {
+                        st_cg_hint(reinterpret_cast<double2 *>(o + y * N), make_double2(v.re, v.im), pol_last);
+                    });
+            }
+            fence_proxy_async_smem();  // these reads before the next item's bulk copies
+            __syncthreads();           // then one cumulative release publishes every thread's stores
+            if (tid == 0) red_release_gpu_add(&ctl->cnt[slot], 1u);
+        } else {
+            // 1. the G y-rows of every plane of the slot (its plane items are done)
+            if (tid == 0) mbar_arrive_expect_tx(&s_bar, (uint32_t)(N * G) * ROW_BYTES);
+            for (int q = tid; q < N * G; q += NT) {
+                const int x = q / G, yl = q % G;
+                fence_proxy_async_global();  // the acquire above precedes these reads
+                bulk_g2s(sm + YG::off(q, 0), sv + ((long long)x * N + it.j * G + yl) * N, ROW_BYTES, &s_bar);
+            }
+            if (!wait_copies()) s_stop = 2;
+            __syncthreads();
+            if (s_stop) break;
+            if (tid == 0) red_release_gpu_add(&ctl->cnt[TWOPASS_RMAX + slot], 1u);
+            // 2. x pass, straight to the output: line = (yl, z)
+            cx<T> *gvol = out + it.vol * TG::V;
+            for (int base = 0; base < LINES; base += WARPS * LS) {
+                const int l = base + warp * LS + lw;
+                const bool valid = l < LINES;
+                const int yl = valid ? l / N : 0, z = l % N;
+                const cx<T> *col = sm + YG::off(yl, z);
+                cx<T> *o = gvol + (long long)(it.j * G + yl) * N + z;
+                lane_split_line<N, P, LS, S, T>(
+                    t, valid, [&](int x) { return col[x * G * PITCH]; },
+                    [&](int x, cx<T> v) {
+                        if constexpr (S > 0) v = cscale(v, scale);
+                        store_out(o + (long long)x * N * N, v);
+                    });
+            }
+            fence_proxy_async_smem();
+            __syncthreads();
+        }
+    }
+    if (copies_pending) mbar_wait_bounded(&s_bar, phase ^ 1u);
+
+    if (tid == 0 && s_stop == 2) {
+        report_error(err, DEV_ERR_DEP_TIMEOUT);
+        atomicExch(&ctl->abort, 1u);
+    }
+    if (tid == 0) {
+        __threadfence();
+        const unsigned prev = atomicAdd(&ctl->done, 1u);
+        if (prev == gridDim.x - 1) {
+            __threadfence();
+            ctl->ticket = 0ull;
+            for (int i = 0; i < 2 * TWOPASS_RMAX; ++i) ctl->cnt[i] = 0u;
+            ctl->abort = 0u;
+            __threadfence();
+            ctl->done = 0u;
+        }
+    }
+}
+
 // TWOPASS for N^3 with every line split into two thread-level stages
 // (staged.cuh: 64 = 8 x 8 Cooley-Tukey, 45 = 5 x 9 Good-Thomas): one plane or
 // one y-row per item, a task holds 5 to 9 points, so many warps fit an SM --
@@ -927,6 +1093,31 @@ static void add_twopass_regs(std::vector<KernelEntry> &out, const char *name)
     add_twopass_regs<N0, N1, N2, +1, G, NT, MINB, true, true>(                                   \
         out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G " bulkq nt" #NT " minb" #MINB)
 
+template <int N, int S, int G, int NT, int MINB, int P>
+static void add_twopass_lanes(std::vector<KernelEntry> &out, const char *name)
+{
+    using TG = TwoPassGeom<N, N, N, double, G, (N | 1)>;
+    KernelEntry e;
+    e.n0 = e.n1 = e.n2 = N;
+    e.precision = FFT3D_B200_C128;
+    e.sign = S;
+    e.family = FAM_TWOPASS;  // same launch arguments and workspace as k_twopass
+    e.alg = 1024 + P;
+    e.vpc = G;
+    e.threads = NT;
+    e.smem = TG::SMEM;
+    e.func = (const void *)&k_twopass_lanes<N, S, G, NT, MINB, P>;
+    e.name = name;
+    out.push_back(e);
+}
+
+// Lines split over P lanes of a warp, lean control: "lanesP" in the name.
+#define FFT3D_TWOPASS_LANES(N, G, NT, MINB, P)                                                    \
+    add_twopass_lanes<N, -1, G, NT, MINB, P>(out, "twopass " #N "x" #N "x" #N " double g" #G      \
+                                                  " lanes" #P " nt" #NT " minb" #MINB);          \
+    add_twopass_lanes<N, +1, G, NT, MINB, P>(out, "twopass " #N "x" #N "x" #N " double g" #G      \
+                                                  " lanes" #P " nt" #NT " minb" #MINB)
+
 template <class Line, int S, int NT, int MINB, typename T = double>
 static void add_twopass_staged(std::vector<KernelEntry> &out, const char *name)
 {
@@ -974,6 +1165,11 @@ static void add_twopass_staged(std::vector<KernelEntry> &out, const char *name)
 
 void register_twopass_kernels(std::vector<KernelEntry> &out)
 {
+    // 36-point lines over 2 lanes (18 points each) or 4 lanes (9 points each)
+    FFT3D_TWOPASS_LANES(36, 2, 160, 3, 2);
+    FFT3D_TWOPASS_LANES(36, 2, 288, 3, 4);
+    FFT3D_TWOPASS_LANES(36, 1, 160, 6, 4);
+    FFT3D_TWOPASS_LANES(36, 3, 448, 2, 4);
     // lean control: next ticket taken ahead, dependency waited at the top
     FFT3D_TWOPASS_BULKQH(36, 36, 36, 3, 128, 3);
     FFT3D_TWOPASS_BULKQH_F(36, 36, 36, 3, 128, 5, 38);

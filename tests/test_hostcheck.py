@@ -202,6 +202,28 @@ def test_twopass_split_lines(hostcheck, shape, prec, g, nvol, sign):
     assert err < (C128_TOL if prec == 0 else C64_TOL), err
 
 
+LANES = [(2, 2, 11), (2, 4, 5), (1, 4, 3), (3, 4, 7)]  # (G, P, batch)
+
+
+@pytest.mark.parametrize("g,p,nvol", LANES, ids=[f"g{t[0]}-lanes{t[1]}-b{t[2]}" for t in LANES])
+@pytest.mark.parametrize("sign", [-1, +1])
+def test_twopass_lane_split(hostcheck, g, p, nvol, sign):
+    """The lane-split TWOPASS kernel for 36^3 complex double (alg = 1024 + P,
+    vpc = G): 36 = 2 x 18 Cooley-Tukey with the lane twiddle, or 4 x 9
+    Good-Thomas, at the kernel's row pitch of 37 and its index maps, in ticket
+    order with the dependency check."""
+    import ctypes
+    hostcheck.hostcheck_twopass_violations.restype = ctypes.c_longlong
+    hostcheck.hostcheck_twopass_violations()
+    shape = (36, 36, 36)
+    rng = np.random.default_rng(8000 + g + 10 * p + nvol)
+    x = field(rng, (nvol,) + shape, dist="normal")
+    got = run(hostcheck, x, shape, 0, sign, 1024 + p, g)
+    assert hostcheck.hostcheck_twopass_violations() == 0
+    want = oracle.fft3d(x) if sign < 0 else oracle.ifft3d(x)
+    assert oracle.rel_error_per_volume(got, want).max() < C128_TOL
+
+
 GOLD = [p for p in sorted(glob.glob(os.path.join(GOLDEN, "vol_*.npz")))]
 
 

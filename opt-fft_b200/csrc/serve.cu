@@ -200,6 +200,7 @@ static void server_loop(fft3d_b200_server *s)
 {
     cudaSetDevice(s->device);
     const bool plain = (s->flags & FFT3D_B200_SERVE_PLAIN) != 0;
+    std::vector<ServeSlot *> to_launch;
     while (true) {
         std::unique_lock<std::mutex> lk(s->mu);
         bool progress = false;
@@ -224,7 +225,8 @@ static void server_loop(fft3d_b200_server *s)
             slot.busy = false;
             progress = true;
         }
-        // admit pending requests, FIFO, into a free slot
+        // admit pending requests, FIFO, into free slots
+        to_launch.clear();
         for (ServeSlot &slot : s->slots) {
             if (s->pending.empty()) break;
             if (slot.busy) continue;
@@ -243,27 +245,32 @@ static void server_loop(fft3d_b200_server *s)
             }
             if (slot.reqs.empty()) break;  // head of queue waits for budget
             s->peak_used = std::max(s->peak_used, s->used);
-            const int st = launch_slot(s, slot);
-            if (st) s->status = st;
             slot.busy = true;
             ++s->batches;
             s->batched_requests += (long long)slot.reqs.size();
+            to_launch.push_back(&slot);
             progress = true;
         }
         s->cv.notify_all();
         bool any_busy = false;
         for (const ServeSlot &slot : s->slots) any_busy |= slot.busy;
         if (s->stop && s->pending.empty() && !any_busy) break;
-        if (!progress) {
-            // nothing to do right now: short sleep while work is on the GPU,
-            // otherwise wait for a submission
-            if (any_busy) {
-                lk.unlock();
-                std::this_thread::sleep_for(std::chrono::microseconds(5));
-            } else {
-                s->cv.wait_for(lk, std::chrono::milliseconds(1));
+        if (!progress && !any_busy) {
+            // idle: wait for a submission
+            s->cv.wait_for(lk, std::chrono::milliseconds(1));
+            continue;
+        }
+        // descriptors and launches outside the lock: submitters are not held up;
+        // the slots are this thread's own until they are retired above
+        lk.unlock();
+        for (ServeSlot *slot : to_launch) {
+            const int st = launch_slot(s, *slot);
+            if (st) {
+                std::lock_guard<std::mutex> g(s->mu);
+                s->status = st;
             }
         }
+        if (!progress) std::this_thread::sleep_for(std::chrono::microseconds(5));
     }
 }
 
@@ -344,8 +351,9 @@ extern "C" int fft3d_b200_server_create(size_t hbm_budget_bytes, int max_infligh
     return FFT3D_B200_OK;
 }
 
-extern "C" int fft3d_b200_server_submit(fft3d_b200_server *s, const fft3d_b200_segment *req,
-                                        unsigned long long *ticket)
+// Queue one request; its latency counts from t_arrival (< 0: now, under the lock).
+static int server_submit_at(fft3d_b200_server *s, const fft3d_b200_segment *req,
+                            unsigned long long *ticket, double t_arrival)
 {
     if (!s || !req) return FFT3D_B200_ERR_INVALID;
     const fft3d_b200_segment &q = *req;
@@ -370,7 +378,7 @@ extern "C" int fft3d_b200_server_submit(fft3d_b200_server *s, const fft3d_b200_s
     {
         std::lock_guard<std::mutex> lk(s->mu);
         r.ticket = s->next_ticket++;
-        r.t_submit = now_s();
+        r.t_submit = t_arrival >= 0.0 ? t_arrival : now_s();
         if (s->submitted == 0) s->t_first = r.t_submit;
         ++s->submitted;
         s->pending.push_back(r);
@@ -380,6 +388,15 @@ extern "C" int fft3d_b200_server_submit(fft3d_b200_server *s, const fft3d_b200_s
     return FFT3D_B200_OK;
 }
 
+extern "C" int fft3d_b200_server_submit(fft3d_b200_server *s, const fft3d_b200_segment *req,
+                                        unsigned long long *ticket)
+{
+    return server_submit_at(s, req, ticket, -1.0);
+}
+
+// Requests with arrival times: latency counts from the scheduled arrival, so a
+// submission delayed behind the server (queueing in the client) is charged to
+// the request, as an open-loop load generator must.
 extern "C" int fft3d_b200_server_submit_many(fft3d_b200_server *s, const fft3d_b200_segment *reqs,
                                              const double *arrival_s, int n,
                                              unsigned long long *tickets)
@@ -387,10 +404,13 @@ extern "C" int fft3d_b200_server_submit_many(fft3d_b200_server *s, const fft3d_b
     if (!s || n < 0 || (n > 0 && !reqs)) return FFT3D_B200_ERR_INVALID;
     const double t0 = now_s();
     for (int k = 0; k < n; ++k) {
-        if (arrival_s)
-            while (now_s() - t0 < arrival_s[k]) {
+        double t_arr = -1.0;
+        if (arrival_s) {
+            t_arr = t0 + arrival_s[k];
+            while (now_s() < t_arr) {
             }
-        const int st = fft3d_b200_server_submit(s, &reqs[k], tickets ? &tickets[k] : nullptr);
+        }
+        const int st = server_submit_at(s, &reqs[k], tickets ? &tickets[k] : nullptr, t_arr);
         if (st) return st;
     }
     return FFT3D_B200_OK;

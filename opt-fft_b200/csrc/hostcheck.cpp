@@ -176,11 +176,10 @@ static void emulate_twopass(const void *vin, void *vout, long long nvol)
 }
 
 // The lean-control TWOPASS variants (k_twopass_regs): z pass in the plane
-// layout; y pass stored straight into the slot (YDIRECT) or in shared memory
-// and copied by rows; x pass loaded straight from the slot or from rows
-// gathered into the row layout (XBULK).  Same tickets, ring and dependency
-// checks as emulate_twopass.
-template <int N0, int N1, int N2, typename T, int S, int G, bool XBULK, bool YDIRECT, int PITCH = 0>
+// layout; y pass stored straight into the slot; x pass loaded straight from
+// the slot or from rows gathered into the row layout (XBULK).  Same tickets,
+// ring and dependency checks as emulate_twopass.
+template <int N0, int N1, int N2, typename T, int S, int G, bool XBULK, int PITCH = 0>
 static void emulate_twopass_regs(const void *vin, void *vout, long long nvol)
 {
     using TG = TwoPassGeom<N0, N1, N2, T, G, PITCH>;
@@ -208,14 +207,7 @@ static void emulate_twopass_regs(const void *vin, void *vout, long long nvol)
             for (int r = 0; r < XG::ROWS; ++r)  // the bulk copy of row r
                 for (int z = 0; z < N2; ++z) sm[XG::off(r, z)] = rows[(long long)r * N2 + z];
             for (int r = 0; r < XG::ROWS; ++r) pass_z<XG, S, ALG_DEFAULT>(sm.data(), r);
-            if (YDIRECT) {
-                for (int l = 0; l < G * N2; ++l) pass_y_store_l2<XG, S>(sm.data(), l, sv, it.j * G);
-            } else {
-                for (int l = 0; l < G * N2; ++l) pass_y<XG, S, ALG_DEFAULT>(sm.data(), l);
-                cx<T> *dst = sv + (long long)it.j * G * N1 * N2;
-                for (int r = 0; r < XG::ROWS; ++r)
-                    for (int z = 0; z < N2; ++z) dst[(long long)r * N2 + z] = sm[XG::off(r, z)];
-            }
+            for (int l = 0; l < G * N2; ++l) pass_y_store_l2<XG, S>(sm.data(), l, sv, it.j * G);
         } else if (XBULK) {
             for (int q = 0; q < N0 * G; ++q) {
                 const int x = q / G, yl = q % G;
@@ -353,97 +345,17 @@ static void emulate_twopass_staged(const void *vin, void *vout, long long nvol)
     }
 }
 
-// The split-line TWOPASS variant (SPLIT = true): every pass whose length has a
-// lane split runs split_line_host over whole lines, the host form of the
-// kernel's lane exchange; other axes keep the one-thread-per-line pass.
-template <int N, int S, typename T, class Ld, class St>
-static void line_any(Ld ld, St st)
-{
-    if constexpr (LineSplit<N>::P > 1) {
-        split_line_host<N, S, T>(ld, st);
-    } else {
-        cx<T> v[N];
-        for (int j = 0; j < N; ++j) v[j] = ld(j);
-        dft<N, S, T>(v);
-        for (int j = 0; j < N; ++j) st(j, v[j]);
-    }
-}
-
-template <int N0, int N1, int N2, typename T, int S, int G>
-static void emulate_twopass_split(const void *vin, void *vout, long long nvol)
-{
-    using TG = TwoPassGeom<N0, N1, N2, T, G>;
-    using XG = typename TG::XG;
-    using YG = typename TG::YG;
-    const T scale = S > 0 ? T(1) / T(TG::V) : T(1);
-    int lag = 0;
-    const int R = twopass_ring_size(TG::NA, TG::NB, 7, &lag);
-    std::vector<cx<T>> sm((size_t)TG::PV), ring((size_t)R * TG::V, cx<T>{T(-777.0), T(555.0)});
-    const cx<T> *in = (const cx<T> *)vin;
-    cx<T> *out = (cx<T> *)vout;
-    const long long total = (long long)(TG::NA + TG::NB) * nvol;
-    for (long long t = 0; t < total; ++t) {
-        const TwoPassItem it = twopass_decode(t, nvol, TG::NA, TG::NB, lag);
-        cx<T> *sv = ring.data() + (it.vol % R) * TG::V;
-        for (auto &e : sm) e = {T(12345.0), T(-6789.0)};
-        cx<T> *s = sm.data();
-        if (it.plane) {
-            for (int g = 0; g < TG::PLANE_ELEMS; ++g) {
-                long long vo;
-                int so;
-                twopass_plane_elem<TG>(it.j, g, &vo, &so);
-                s[so] = in[it.vol * TG::V + vo];
-            }
-            for (int r = 0; r < XG::ROWS; ++r)
-                line_any<N2, S, T>([&](int z) { return s[XG::off(r, z)]; },
-                                   [&](int z, cx<T> v) { s[XG::off(r, z)] = v; });
-            for (int l = 0; l < G * N2; ++l) {
-                const int z = l % N2, rb = (l / N2) * N1;
-                line_any<N1, S, T>([&](int y) { return s[XG::off(rb + y, z)]; },
-                                   [&](int y, cx<T> v) { s[XG::off(rb + y, z)] = v; });
-            }
-            for (int g = 0; g < TG::PLANE_ELEMS; ++g) {
-                long long vo;
-                int so;
-                twopass_plane_elem<TG>(it.j, g, &vo, &so);
-                sv[vo] = s[so];
-            }
-        } else {
-            for (int g = 0; g < TG::ROW_ELEMS; ++g) {
-                long long vo;
-                int so;
-                twopass_row_elem<TG>(it.j, g, &vo, &so);
-                s[so] = sv[vo];
-            }
-            cx<T> *gvol = out + it.vol * TG::V;
-            for (int l = 0; l < G * N2; ++l) {
-                const int z = l % N2, y = l / N2;
-                line_any<N0, S, T>([&](int j) { return s[YG::off(j * G + y, z)]; },
-                                   [&](int j, cx<T> v) {
-                                       if (S > 0) v = cscale(v, scale);
-                                       gvol[((long long)j * N1 + it.j * G + y) * N2 + z] = v;
-                                   });
-            }
-        }
-    }
-}
 
 typedef void (*emu_fn)(const void *, void *, long long);
 
-#define EMU_TPS(N0, N1, N2, T, G)                                                             \
-    {N0, N1, N2, sizeof(T) == 8 ? 0 : 1, -1, 400 + G, 1,                                    \
-     &emulate_twopass_split<N0, N1, N2, T, -1, G>},                                          \
-    {N0, N1, N2, sizeof(T) == 8 ? 0 : 1, +1, 400 + G, 1, &emulate_twopass_split<N0, N1, N2, T, +1, G>}
-
-#define EMU_TPR_(N0, N1, N2, G, A, XB, YD)                                                   \
-    {N0, N1, N2, 0, -1, A + G, 1, &emulate_twopass_regs<N0, N1, N2, double, -1, G, XB, YD>},   \
-    {N0, N1, N2, 0, +1, A + G, 1, &emulate_twopass_regs<N0, N1, N2, double, +1, G, XB, YD>}
-#define EMU_TPR(N0, N1, N2, G) EMU_TPR_(N0, N1, N2, G, 500, false, true)
-#define EMU_TPRP(N0, N1, N2, G) EMU_TPR_(N0, N1, N2, G, 520, true, false)
-#define EMU_TPRQ(N0, N1, N2, G) EMU_TPR_(N0, N1, N2, G, 540, true, true)
+#define EMU_TPR_(N0, N1, N2, G, A, XB)                                                       \
+    {N0, N1, N2, 0, -1, A + G, 1, &emulate_twopass_regs<N0, N1, N2, double, -1, G, XB>},       \
+    {N0, N1, N2, 0, +1, A + G, 1, &emulate_twopass_regs<N0, N1, N2, double, +1, G, XB>}
+#define EMU_TPR(N0, N1, N2, G) EMU_TPR_(N0, N1, N2, G, 500, false)
+#define EMU_TPRQ(N0, N1, N2, G) EMU_TPR_(N0, N1, N2, G, 540, true)
 #define EMU_TPRQF(G)                                                                          \
-    {36, 36, 36, 1, -1, 540 + G, 1, &emulate_twopass_regs<36, 36, 36, float, -1, G, true, true, 38>},  \
-    {36, 36, 36, 1, +1, 540 + G, 1, &emulate_twopass_regs<36, 36, 36, float, +1, G, true, true, 38>}
+    {36, 36, 36, 1, -1, 540 + G, 1, &emulate_twopass_regs<36, 36, 36, float, -1, G, true, 38>},  \
+    {36, 36, 36, 1, +1, 540 + G, 1, &emulate_twopass_regs<36, 36, 36, float, +1, G, true, 38>}
 #define EMU_TPL(N, G, P)                                                                      \
     {N, N, N, 0, -1, 1024 + P, G, &emulate_twopass_lanes<N, -1, G, P>},                        \
     {N, N, N, 0, +1, 1024 + P, G, &emulate_twopass_lanes<N, +1, G, P>}
@@ -494,11 +406,8 @@ static const EmuEntry kEmu[] = {
     EMU(13, 13, 13, double, 0, 2), EMU(23, 23, 23, double, 0, 1),  EMU(13, 13, 13, float, 0, 4),
     EMU(23, 23, 23, float, 0, 1),  EMU_TP(45, 45, 45, double, 3), EMU_TP(45, 45, 45, float, 5),
     EMU_TP(64, 64, 64, double, 1), EMU_TP(64, 64, 64, float, 2),
-    EMU_TPS(36, 36, 36, double, 2), EMU_TPS(36, 36, 36, double, 1), EMU_TPS(36, 36, 36, float, 4),
-    EMU_TPS(64, 64, 64, double, 1), EMU_TPS(64, 64, 64, float, 2),  EMU_TPS(36, 36, 64, double, 2),
-    EMU_TPR(36, 36, 36, 3), EMU_TPR(36, 36, 36, 2), EMU_TPR(36, 36, 36, 4), EMU_TPRP(36, 36, 36, 3), EMU_TPRP(36, 36, 36, 2), EMU_TPRQ(36, 36, 36, 3),
-    EMU_TPRQ(36, 36, 36, 2), EMU_TPRP(45, 45, 45, 3), EMU_TPRP(6, 9, 5, 3), EMU_TPRQ(6, 9, 5, 3), EMU_TPRQF(3), EMU_TPRQF(2), EMU_TPRQF(4), EMU_TPST(LineCT64, 64, double), EMU_TPST(LineCT64, 64, float), EMU_TPST(LinePFA45, 45, double),
-    EMU_TPST(LinePFA36, 36, double), EMU_TPST(LinePFA36, 36, float),
+    EMU_TPR(36, 36, 36, 3), EMU_TPR(36, 36, 36, 2), EMU_TPR(36, 36, 36, 4), EMU_TPRQ(36, 36, 36, 3),
+    EMU_TPRQ(36, 36, 36, 2), EMU_TPRQ(6, 9, 5, 3), EMU_TPRQF(3), EMU_TPRQF(2), EMU_TPRQF(4), EMU_TPST(LineCT64, 64, double), EMU_TPST(LineCT64, 64, float), EMU_TPST(LinePFA45, 45, double),
     EMU_TPR(6, 9, 5, 3),
     EMU_TPL(36, 2, 2), EMU_TPL(36, 2, 4), EMU_TPL(36, 1, 4), EMU_TPL(36, 3, 4),
     // the group sizes the VOLUME kernels of these extents use

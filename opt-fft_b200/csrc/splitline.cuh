@@ -1,12 +1,14 @@
 // splitline.cuh -- a line of N = P*Q points transformed by P lanes of one warp.
 //
-// A 36- or 64-point complex-double line held by one thread needs 170-260
-// registers, which caps a kernel at a few warps per SM and spills.  Here lane t
-// of the P lanes (P consecutive lanes of a warp) holds Q = N/P points:
+// A line longer than one thread can hold in registers (the multi-GPU path's
+// 96- to 256-point lines; 36-point complex-double lines, 170 registers in one
+// thread, for the lane-split TWOPASS kernel) is spread over P lanes.  Lane t of
+// the P lanes (P consecutive lanes of a warp for LineSplit, lanes LS apart for
+// LaneSplit below) holds Q = N/P points:
 //   1. it loads its points n = in(t, n2), n2 = 0..Q-1, and runs a Q-point DFT;
 //   2. Cooley-Tukey splits (P, Q not coprime) multiply by W_N^(t*k2);
 //   3. a P-point DFT across the P lanes, radix-2 decimation in frequency with
-//      __shfl_xor_sync (lane distance P/2, ..., 1), leaves lane t with
+//      __shfl_xor_sync (lane distance P/2, ..., 1, times LS), leaves lane t with
 //      frequency k1 = bitrev(t) of every k2;
 //   4. it stores its Q results at k = out(k1, k2).
 // Prime-factor splits (gcd(P, Q) = 1) use the Good-Thomas maps
@@ -25,16 +27,6 @@ namespace fft3d {
 template <int N>
 struct LineSplit {
     static constexpr int P = 1;
-};
-template <>
-struct LineSplit<36> {
-    static constexpr int P = 4, Q = 9;
-    static constexpr bool PFA = true;
-};
-template <>
-struct LineSplit<64> {
-    static constexpr int P = 4, Q = 16;
-    static constexpr bool PFA = false;
 };
 // Lines longer than one thread can hold (the multi-GPU large cubes).
 template <>

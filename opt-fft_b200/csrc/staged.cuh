@@ -18,7 +18,6 @@
 #pragma once
 
 #include "codelets.cuh"
-#include "pfa36.cuh"
 
 namespace fft3d {
 
@@ -111,26 +110,6 @@ struct LinePFA45 {
         dft<9, S, T>(v);
 #pragma unroll
         for (int k2 = 0; k2 < 9; ++k2) store(line, (36 * k1 + 10 * k2) % 45, v[k2]);
-    }
-};
-
-// 36 = 4 x 9 Good-Thomas (pfa36.cuh): the second stage's outputs of class k1
-// fill exactly the slots its inputs came from, so X[k] is stored in slot k.
-struct LinePFA36 {
-    static constexpr int N = 36, T1 = 9, T2 = 4;
-    FFT_HD static constexpr int slot(int k) { return k; }
-    FFT_HD static constexpr int at(int p) { return p; }
-
-    template <int S, typename T, class Addr>
-    FFT_HD static void stage1(cx<T> *sm, int lines, int t, Addr addr)
-    {
-        pfa36_stage1<S, T>(sm, lines, t, addr);
-    }
-
-    template <int S, typename T, class Addr, class Store>
-    FFT_HD static void stage2(const cx<T> *sm, int lines, int t, Addr addr, Store store)
-    {
-        pfa36_stage2<S, T>(sm, lines, t, addr, store);
     }
 };
 

@@ -49,87 +49,7 @@ __device__ __forceinline__ void st_l2(cx<T> *p, cx<T> v)
     else __stcg(reinterpret_cast<float2 *>(p), make_float2(v.re, v.im));
 }
 
-// The three passes with each line spread over P = LineSplit<N>::P lanes
-// (splitline.cuh); axes whose length has no split keep one thread per line.
-// Every lane of the CTA runs the same number of rounds, so whole warps reach
-// each shuffle; P consecutive tasks are the P lanes of one line.
-template <class XG, int S, int NT>
-__device__ __forceinline__ void tp_pass_z(cx<typename XG::T> *sm, int tid)
-{
-    using T = typename XG::T;
-    constexpr int N = XG::N2, P = LineSplit<N>::P;
-    if constexpr (P == 1) {
-        for (int r = tid; r < XG::ROWS; r += NT) pass_z<XG, S, ALG_DEFAULT>(sm, r);
-    } else {
-        static_assert(NT % 32 == 0, "whole warps");
-        constexpr int TASKS = XG::ROWS * P;
-        for (int base = 0; base < TASKS; base += NT) {
-            const int task = base + tid;
-            const bool valid = task < TASKS;
-            const int r = valid ? task / P : 0, t = task % P;
-            split_line<N, S, T>(t, valid, [&](int z) { return sm[XG::off(r, z)]; },
-                                [&](int z, cx<T> v) { sm[XG::off(r, z)] = v; });
-        }
-    }
-}
-
-template <class XG, int S, int NT>
-__device__ __forceinline__ void tp_pass_y(cx<typename XG::T> *sm, int tid)
-{
-    using T = typename XG::T;
-    constexpr int N = XG::N1, P = LineSplit<N>::P;
-    constexpr int LINES = XG::N0 * XG::N2;
-    if constexpr (P == 1) {
-        for (int l = tid; l < LINES; l += NT) pass_y<XG, S, ALG_DEFAULT>(sm, l);
-    } else {
-        static_assert(NT % 32 == 0, "whole warps");
-        constexpr int TASKS = LINES * P;
-        for (int base = 0; base < TASKS; base += NT) {
-            const int task = base + tid;
-            const bool valid = task < TASKS;
-            const int l = valid ? task / P : 0, t = task % P;
-            const int z = l % XG::N2, rb = (l / XG::N2) * XG::N1;
-            split_line<N, S, T>(t, valid, [&](int y) { return sm[XG::off(rb + y, z)]; },
-                                [&](int y, cx<T> v) { sm[XG::off(rb + y, z)] = v; });
-        }
-    }
-}
-
-// x pass of a row item: YG holds G y-rows of all N0 planes; results go to gvol.
-template <class YG, int S, int GN1, int NT>
-__device__ __forceinline__ void tp_pass_x(const cx<typename YG::T> *sm, int tid, cx<typename YG::T> *gvol,
-                                          int y0, typename YG::T scale)
-{
-    using T = typename YG::T;
-    constexpr int N = YG::N0, P = LineSplit<N>::P;
-    constexpr int LINES = YG::N1 * YG::N2;
-    if constexpr (P == 1) {
-        for (int l = tid; l < LINES; l += NT) pass_x_slab<YG, S, GN1>(sm, l, gvol, y0, scale);
-    } else {
-        static_assert(NT % 32 == 0, "whole warps");
-        constexpr int TASKS = LINES * P;
-        for (int base = 0; base < TASKS; base += NT) {
-            const int task = base + tid;
-            const bool valid = task < TASKS;
-            const int l = valid ? task / P : 0, t = task % P;
-            const int z = l % YG::N2, y = l / YG::N2;
-            split_line<N, S, T>(
-                t, valid, [&](int j) { return sm[YG::off(j * YG::N1 + y, z)]; },
-                [&](int j, cx<T> v) {
-                    if constexpr (S > 0) v = cscale(v, scale);
-                    store_out(gvol + ((long long)j * GN1 + y0 + y) * YG::N2 + z, v);
-                });
-        }
-    }
-}
-
-// BULK (complex double): every row of N2 points is moved by one bulk copy
-// (cp.async.bulk, completing on an mbarrier with a bounded wait) -- the plane
-// rows from the input, the row-item rows from scratch -- and the scratch store
-// walks whole rows, one warp per row: no per-element index arithmetic, which
-// otherwise costs more instructions than the transform itself.
-template <int N0, int N1, int N2, typename T, int S, int G, int NT, int MINB, bool SPLIT,
-          bool BULK = false>
+template <int N0, int N1, int N2, typename T, int S, int G, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB)
     k_twopass(const cx<T> *__restrict__ in, cx<T> *__restrict__ out, long long nvol, T scale,
               int *err, unsigned char *work, int R, int D)
@@ -138,28 +58,15 @@ __global__ void __launch_bounds__(NT, MINB)
     using TG = TwoPassGeom<N0, N1, N2, T, G>;
     using XG = typename TG::XG;
     using YG = typename TG::YG;
-    static_assert(!BULK || (sizeof(T) == 8 && XG::POL != 2 && NT % 32 == 0),
-                  "bulk rows: complex double, row-major layouts, whole warps");
     constexpr int U = 8;  // L2 loads in flight per thread in the row gather
-    constexpr uint32_t ROW_BYTES = (uint32_t)(N2 * sizeof(cx<T>));
     extern __shared__ __align__(16) unsigned char smraw[];
     cx<T> *sm = reinterpret_cast<cx<T> *>(smraw);
     __shared__ long long s_t;
     __shared__ int s_stop;
-    __shared__ __align__(8) uint64_t s_bar;
     TwoPassCtl *ctl = reinterpret_cast<TwoPassCtl *>(work);
     cx<T> *ring = reinterpret_cast<cx<T> *>(work + TWOPASS_CTL_BYTES);
     const int tid = threadIdx.x;
     const long long total = (long long)(TG::NA + TG::NB) * nvol;
-    uint32_t phase = 0;
-    bool copies_pending = false;
-    if constexpr (BULK) {
-        if (tid == 0) {
-            mbar_init(&s_bar, 1);
-            fence_mbar_init();
-        }
-        __syncthreads();
-    }
 
     for (;;) {
         if (tid == 0) {
@@ -177,40 +84,20 @@ __global__ void __launch_bounds__(NT, MINB)
         if (it.plane) {
             // 1. G contiguous planes of the input
             const cx<T> *src = in + it.vol * TG::V;
-            if constexpr (BULK) {
-                if (tid == 0) mbar_arrive_expect_tx(&s_bar, (uint32_t)XG::ROWS * ROW_BYTES);
-                const cx<T> *rows = src + (long long)it.j * G * N1 * N2;
-                for (int r = tid; r < XG::ROWS; r += NT)
-                    bulk_g2s(sm + XG::off(r, 0), rows + (long long)r * N2, ROW_BYTES, &s_bar);
-                copies_pending = true;
-                const bool ok = mbar_wait_bounded(&s_bar, phase);
-                phase ^= 1u;
-                if (!ok && tid == 0) s_stop = 2;
-                if (ok) copies_pending = false;
-                __syncthreads();
-                if (s_stop) break;
-            } else {
-                for (int g = tid; g < TG::PLANE_ELEMS; g += NT) {
-                    long long vo;
-                    int so;
-                    twopass_plane_elem<TG>(it.j, g, &vo, &so);
-                    if constexpr (sizeof(T) == 8) cp_async_16(sm + so, src + vo);
-                    else cp_async_8(sm + so, src + vo);
-                }
-                cp_async_commit();
-                cp_async_wait<0>();
-                __syncthreads();
+            for (int g = tid; g < TG::PLANE_ELEMS; g += NT) {
+                long long vo;
+                int so;
+                twopass_plane_elem<TG>(it.j, g, &vo, &so);
+                if constexpr (sizeof(T) == 8) cp_async_16(sm + so, src + vo);
+                else cp_async_8(sm + so, src + vo);
             }
+            cp_async_commit();
+            cp_async_wait<0>();
+            __syncthreads();
             // 2. z and y passes
-            if constexpr (SPLIT) {
-                tp_pass_z<XG, S, NT>(sm, tid);
-                __syncthreads();
-                tp_pass_y<XG, S, NT>(sm, tid);
-            } else {
-                for (int r = tid; r < G * N1; r += NT) pass_z<XG, S, ALG_DEFAULT>(sm, r);
-                __syncthreads();
-                for (int l = tid; l < G * N2; l += NT) pass_y<XG, S, ALG_DEFAULT>(sm, l);
-            }
+            for (int r = tid; r < G * N1; r += NT) pass_z<XG, S, ALG_DEFAULT>(sm, r);
+            __syncthreads();
+            for (int l = tid; l < G * N2; l += NT) pass_y<XG, S, ALG_DEFAULT>(sm, l);
             // 3. the slot's previous volume must have been read out
             if (tid == 0)
                 s_stop = wait_counter_geq(&ctl->cnt[TWOPASS_RMAX + slot], (unsigned)TG::NB * round,
@@ -220,17 +107,11 @@ __global__ void __launch_bounds__(NT, MINB)
             __syncthreads();
             if (s_stop) break;
             // 4. to scratch, same offsets as in the volume, L2 only
-            if constexpr (BULK) {
-                cx<T> *rows = sv + (long long)it.j * G * N1 * N2;
-                for (int r = tid / 32; r < XG::ROWS; r += NT / 32)
-                    for (int z = tid % 32; z < N2; z += 32) st_l2(rows + (long long)r * N2 + z, sm[XG::off(r, z)]);
-            } else {
-                for (int g = tid; g < TG::PLANE_ELEMS; g += NT) {
-                    long long vo;
-                    int so;
-                    twopass_plane_elem<TG>(it.j, g, &vo, &so);
-                    st_l2(sv + vo, sm[so]);
-                }
+            for (int g = tid; g < TG::PLANE_ELEMS; g += NT) {
+                long long vo;
+                int so;
+                twopass_plane_elem<TG>(it.j, g, &vo, &so);
+                st_l2(sv + vo, sm[so]);
             }
             __syncthreads();  // then one cumulative release publishes every thread's stores
             if (tid == 0) red_release_gpu_add(&ctl->cnt[slot], 1u);
@@ -243,22 +124,6 @@ __global__ void __launch_bounds__(NT, MINB)
             __syncthreads();
             if (s_stop) break;
             // 2. gather the G rows of every plane
-            if constexpr (BULK) {
-                if (tid == 0) mbar_arrive_expect_tx(&s_bar, (uint32_t)(N0 * G) * ROW_BYTES);
-                for (int q = tid; q < N0 * G; q += NT) {
-                    const int x = q / G, yl = q % G;
-                    fence_proxy_async_global();  // the acquire above precedes these TMA reads
-                    bulk_g2s(sm + YG::off(q, 0), sv + ((long long)x * N1 + it.j * G + yl) * N2, ROW_BYTES,
-                             &s_bar);
-                }
-                copies_pending = true;
-                const bool ok = mbar_wait_bounded(&s_bar, phase);
-                phase ^= 1u;
-                if (!ok && tid == 0) s_stop = 2;
-                if (ok) copies_pending = false;
-                __syncthreads();
-                if (s_stop) break;
-            } else
             for (int base = 0; base < TG::ROW_ELEMS; base += NT * U) {
                 cx<T> v[U];
                 int so[U];
@@ -281,16 +146,9 @@ __global__ void __launch_bounds__(NT, MINB)
             if (tid == 0) red_release_gpu_add(&ctl->cnt[TWOPASS_RMAX + slot], 1u);
             // 3. x pass, straight to the output
             cx<T> *gvol = out + it.vol * TG::V;
-            if constexpr (SPLIT) tp_pass_x<YG, S, N1, NT>(sm, tid, gvol, it.j * G, scale);
-            else
-                for (int l = tid; l < G * N2; l += NT) pass_x_slab<YG, S, N1>(sm, l, gvol, it.j * G, scale);
+            for (int l = tid; l < G * N2; l += NT) pass_x_slab<YG, S, N1>(sm, l, gvol, it.j * G, scale);
         }
-        if constexpr (BULK) fence_proxy_async_smem();  // generic reads before the next TMA writes
         __syncthreads();  // the next item reuses shared memory
-    }
-    // a bulk copy that timed out may still land: wait once more (bounded)
-    if constexpr (BULK) {
-        if (copies_pending) mbar_wait_bounded(&s_bar, phase ^ 1u);
     }
 
     // A wait that timed out: record it and stop the other CTAs.
@@ -466,14 +324,14 @@ __global__ void __launch_bounds__(NT, MINB)
 // ticket-order argument against deadlock still holds.
 //
 // Plane items move their G planes into shared memory by bulk copies and run
-// the z pass there.  The y pass either stores straight into the scratch slot
-// from registers (YDIRECT, L2-only stores; "regs"/"bulkq" in the name) or runs
-// in shared memory, whose rows then go to the slot one warp per row ("bulkp").
-// Row items either load their x-lines straight from the slot into registers
-// (L2-only loads, a warp reading contiguous ranges; no shared memory at all,
-// "regs") or gather their rows by bulk copies first (XBULK, "bulkp"/"bulkq").
+// the z pass there; the y pass stores straight into the scratch slot from
+// registers (L2-only stores).  Row items either load their x-lines straight
+// from the slot into registers (L2-only loads, a warp reading contiguous
+// ranges; no shared memory at all, "regs" in the name) or gather their rows by
+// bulk copies first (XBULK, "bulkqh").  HINT adds the L2 policies: input rows
+// evict_first, ring stores evict_last.
 template <int N0, int N1, int N2, int S, int G, int NT, int MINB, bool XBULK = false,
-          bool YDIRECT = true, bool HINT = false, typename T = double, int PITCH = 0>
+          bool HINT = false, typename T = double, int PITCH = 0>
 __global__ void __launch_bounds__(NT, MINB)
     k_twopass_regs(const cx<T> *__restrict__ in, cx<T> *__restrict__ out, long long nvol, T scale,
                    int *err, unsigned char *work, int R, int D)
@@ -561,7 +419,7 @@ __global__ void __launch_bounds__(NT, MINB)
             for (int r = tid; r < XG::ROWS; r += NT) pass_z<XG, S, ALG_DEFAULT>(sm, r);
             __syncthreads();
             // 3. y pass into the scratch slot (its previous reader is done: checked in step 1)
-            if constexpr (YDIRECT && HINT) {
+            if constexpr (HINT) {
                 // ring lines stay in L2 (evict_last): a slot is rewritten in L2, not written back
                 for (int l = tid; l < G * N2; l += NT) {
                     const int z = l % N2, g = l / N2;
@@ -578,14 +436,8 @@ __global__ void __launch_bounds__(NT, MINB)
                             st_cg_hint(reinterpret_cast<float2 *>(o + j * N2), make_float2(v[j].re, v[j].im), pol_last);
                     }
                 }
-            } else if constexpr (YDIRECT) {
-                for (int l = tid; l < G * N2; l += NT) pass_y_store_l2<XG, S>(sm, l, sv, it.j * G);
             } else {
-                for (int l = tid; l < G * N2; l += NT) pass_y<XG, S, ALG_DEFAULT>(sm, l);
-                __syncthreads();
-                cx<T> *dst = sv + (long long)it.j * G * N1 * N2;
-                for (int r = tid / 32; r < XG::ROWS; r += NT / 32)
-                    for (int z = tid % 32; z < N2; z += 32) store_l2(dst + (long long)r * N2 + z, sm[XG::off(r, z)]);
+                for (int l = tid; l < G * N2; l += NT) pass_y_store_l2<XG, S>(sm, l, sv, it.j * G);
             }
             fence_proxy_async_smem();  // these reads before the next item's bulk copies
             __syncthreads();  // then one cumulative release publishes every thread's stores
@@ -992,8 +844,7 @@ size_t entry_workspace_bytes(const KernelEntry &e, int grid_limit)
     return TWOPASS_CTL_BYTES + (size_t)r * (size_t)e.n0 * e.n1 * e.n2 * (size_t)element_bytes(e.precision);
 }
 
-template <int N0, int N1, int N2, typename T, int S, int G, int NT, int MINB, bool SPLIT = false,
-          bool BULK = false>
+template <int N0, int N1, int N2, typename T, int S, int G, int NT, int MINB>
 static void add_twopass(std::vector<KernelEntry> &out, const char *name)
 {
     KernelEntry e;
@@ -1006,8 +857,8 @@ static void add_twopass(std::vector<KernelEntry> &out, const char *name)
     e.vpc = G;
     e.threads = NT;
     e.smem = TwoPassGeom<N0, N1, N2, T, G>::SMEM;
-    e.alg = (SPLIT ? 1 : 0) + (BULK ? 4 : 0);
-    e.func = (const void *)&k_twopass<N0, N1, N2, T, S, G, NT, MINB, SPLIT, BULK>;
+    e.alg = 0;
+    e.func = (const void *)&k_twopass<N0, N1, N2, T, S, G, NT, MINB>;
     e.name = name;
     out.push_back(e);
 }
@@ -1037,7 +888,7 @@ static void add_twopass_pipe(std::vector<KernelEntry> &out, const char *name)
     out.push_back(e);
 }
 
-template <int N0, int N1, int N2, int S, int G, int NT, int MINB, bool XBULK = false, bool YDIRECT = true,
+template <int N0, int N1, int N2, int S, int G, int NT, int MINB, bool XBULK = false,
           bool HINT = false, typename T = double, int PITCH = 0>
 static void add_twopass_regs(std::vector<KernelEntry> &out, const char *name)
 {
@@ -1050,12 +901,12 @@ static void add_twopass_regs(std::vector<KernelEntry> &out, const char *name)
     e.precision = sizeof(T) == 8 ? FFT3D_B200_C128 : FFT3D_B200_C64;
     e.sign = S;
     e.family = FAM_TWOPASS;  // same launch arguments and workspace as k_twopass
-    e.alg = 8 + (XBULK ? 32 : 0) + (YDIRECT ? 0 : 64) + (HINT ? 128 : 0);
+    e.alg = 8 + (XBULK ? 32 : 0) + (HINT ? 128 : 0);
     e.vpc = G;
     e.threads = NT;
     // plane items only, unless row items gather their rows into shared memory too
     e.smem = XBULK ? TG::SMEM : ((XG::PV * XG::EB) + 127) / 128 * 128;
-    e.func = (const void *)&k_twopass_regs<N0, N1, N2, S, G, NT, MINB, XBULK, YDIRECT, HINT, T, PITCH>;
+    e.func = (const void *)&k_twopass_regs<N0, N1, N2, S, G, NT, MINB, XBULK, HINT, T, PITCH>;
     e.name = name;
     out.push_back(e);
 }
@@ -1067,31 +918,20 @@ static void add_twopass_regs(std::vector<KernelEntry> &out, const char *name)
     add_twopass_regs<N0, N1, N2, +1, G, NT, MINB>(out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G \
                                                        " regs nt" #NT " minb" #MINB)
 
-// Lean control with bulk row gathers: "bulkp" (y pass in shared memory, rows
-// stored by warps) and "bulkq" (y pass stored from registers).
-#define FFT3D_TWOPASS_BULKP(N0, N1, N2, G, NT, MINB)                                             \
-    add_twopass_regs<N0, N1, N2, -1, G, NT, MINB, true, false>(                                  \
-        out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G " bulkp nt" #NT " minb" #MINB);       \
-    add_twopass_regs<N0, N1, N2, +1, G, NT, MINB, true, false>(                                  \
-        out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G " bulkp nt" #NT " minb" #MINB)
-// bulkq with L2 policies: input planes evict_first, ring stores evict_last ("bulkqh").
+// Lean control, bulk row gathers, L2 policies: input planes evict_first, ring stores
+// evict_last ("bulkqh").
 #define FFT3D_TWOPASS_BULKQH(N0, N1, N2, G, NT, MINB)                                            \
-    add_twopass_regs<N0, N1, N2, -1, G, NT, MINB, true, true, true>(                             \
+    add_twopass_regs<N0, N1, N2, -1, G, NT, MINB, true, true>(                             \
         out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G " bulkqh nt" #NT " minb" #MINB);      \
-    add_twopass_regs<N0, N1, N2, +1, G, NT, MINB, true, true, true>(                             \
+    add_twopass_regs<N0, N1, N2, +1, G, NT, MINB, true, true>(                             \
         out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G " bulkqh nt" #NT " minb" #MINB)
 // bulkqh for complex float at an explicit even row pitch (bulk rows need
 // 16-byte aligned shared-memory starts): "bulkqh" with "float" in the name.
 #define FFT3D_TWOPASS_BULKQH_F(N0, N1, N2, G, NT, MINB, PITCH)                                    \
-    add_twopass_regs<N0, N1, N2, -1, G, NT, MINB, true, true, true, float, PITCH>(                \
+    add_twopass_regs<N0, N1, N2, -1, G, NT, MINB, true, true, float, PITCH>(                \
         out, "twopass " #N0 "x" #N1 "x" #N2 " float g" #G " bulkqh nt" #NT " minb" #MINB);        \
-    add_twopass_regs<N0, N1, N2, +1, G, NT, MINB, true, true, true, float, PITCH>(                \
+    add_twopass_regs<N0, N1, N2, +1, G, NT, MINB, true, true, float, PITCH>(                \
         out, "twopass " #N0 "x" #N1 "x" #N2 " float g" #G " bulkqh nt" #NT " minb" #MINB)
-#define FFT3D_TWOPASS_BULKQ(N0, N1, N2, G, NT, MINB)                                             \
-    add_twopass_regs<N0, N1, N2, -1, G, NT, MINB, true, true>(                                   \
-        out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G " bulkq nt" #NT " minb" #MINB);       \
-    add_twopass_regs<N0, N1, N2, +1, G, NT, MINB, true, true>(                                   \
-        out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G " bulkq nt" #NT " minb" #MINB)
 
 template <int N, int S, int G, int NT, int MINB, int P>
 static void add_twopass_lanes(std::vector<KernelEntry> &out, const char *name)
@@ -1142,13 +982,6 @@ static void add_twopass_staged(std::vector<KernelEntry> &out, const char *name)
     add_twopass_staged<LINE, +1, NT, MINB, T>(out, "twopass " #N "x" #N "x" #N " " #T " g1 " KIND  \
                                                    " nt" #NT " minb" #MINB)
 
-// Rows moved by bulk copies (complex double, row-major layouts): "bulk" in the name.
-#define FFT3D_TWOPASS_BULK(N0, N1, N2, G, NT, MINB)                                              \
-    add_twopass<N0, N1, N2, double, -1, G, NT, MINB, false, true>(                               \
-        out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G " bulk nt" #NT " minb" #MINB);        \
-    add_twopass<N0, N1, N2, double, +1, G, NT, MINB, false, true>(                               \
-        out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G " bulk nt" #NT " minb" #MINB)
-
 // Two-stage pipeline, complex double: "pipe" in the name.
 #define FFT3D_TWOPASS_PIPE(N0, N1, N2, G, NT, MINB)                                              \
     add_twopass_pipe<N0, N1, N2, -1, G, NT, MINB>(out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G \
@@ -1156,90 +989,34 @@ static void add_twopass_staged(std::vector<KernelEntry> &out, const char *name)
     add_twopass_pipe<N0, N1, N2, +1, G, NT, MINB>(out, "twopass " #N0 "x" #N1 "x" #N2 " double g" #G \
                                                        " pipe nt" #NT " minb" #MINB)
 
-// Lines split over P lanes (splitline.cuh): "split" in the name.
-#define FFT3D_TWOPASS_SPLIT(N0, N1, N2, T, G, NT, MINB)                                          \
-    add_twopass<N0, N1, N2, T, -1, G, NT, MINB, true>(out, "twopass " #N0 "x" #N1 "x" #N2 " " #T \
-                                                           " g" #G " split nt" #NT " minb" #MINB); \
-    add_twopass<N0, N1, N2, T, +1, G, NT, MINB, true>(out, "twopass " #N0 "x" #N1 "x" #N2 " " #T \
-                                                           " g" #G " split nt" #NT " minb" #MINB)
-
+// The candidates the autotuner races.  Measured on B200 (forward, in the
+// tuner's race): every variant kept here wins, or comes within a few per cent
+// of the winner, at some batch size -- 4, 16 or 256 volumes of 36^3, 128 of
+// 45^3, 64 of 64^3 -- or is the only kernel for its extent and precision.
 void register_twopass_kernels(std::vector<KernelEntry> &out)
 {
-    // 36-point lines over 2 lanes (18 points each) or 4 lanes (9 points each)
-    FFT3D_TWOPASS_LANES(36, 2, 160, 3, 2);
-    FFT3D_TWOPASS_LANES(36, 2, 288, 3, 4);
-    FFT3D_TWOPASS_LANES(36, 1, 160, 6, 4);
-    FFT3D_TWOPASS_LANES(36, 3, 448, 2, 4);
-    // lean control: next ticket taken ahead, dependency waited at the top
+    // 36^3 complex double: one line per thread, lean control, bulk rows, L2
+    // policies (256 volumes: 124 us); lines over 4 lanes (4 and 16 volumes)
     FFT3D_TWOPASS_BULKQH(36, 36, 36, 3, 128, 3);
+    FFT3D_TWOPASS_BULKQH(36, 36, 36, 2, 96, 4);
+    FFT3D_TWOPASS_LANES(36, 2, 288, 3, 4);
+    FFT3D_TWOPASS_REGS(36, 36, 36, 2, 96, 3);
+    FFT3D_TWOPASS_PIPE(36, 36, 36, 2, 96, 2);
+    // 36^3 complex float at an explicit even row pitch of 38
     FFT3D_TWOPASS_BULKQH_F(36, 36, 36, 3, 128, 5, 38);
     FFT3D_TWOPASS_BULKQH_F(36, 36, 36, 2, 96, 6, 38);
     FFT3D_TWOPASS_BULKQH_F(36, 36, 36, 4, 160, 3, 38);
-    FFT3D_TWOPASS_BULKQH(45, 45, 45, 3, 160, 2);
+    // 45^3: complex double five planes per item; 45 = 5 x 9 staged lines
     FFT3D_TWOPASS_BULKQH(45, 45, 45, 5, 256, 1);
-    FFT3D_TWOPASS_BULKQH(36, 36, 36, 2, 96, 4);
-    FFT3D_TWOPASS_BULKP(36, 36, 36, 3, 128, 3);
-    FFT3D_TWOPASS_BULKP(36, 36, 36, 2, 96, 4);
-    FFT3D_TWOPASS_BULKQ(36, 36, 36, 3, 128, 3);
-    FFT3D_TWOPASS_BULKQ(36, 36, 36, 2, 96, 4);
-    FFT3D_TWOPASS_BULKP(45, 45, 45, 3, 160, 2);
-    // 64-point lines as 8 x 8 stages: one plane or y-row per item
-    FFT3D_TWOPASS_STAGED(LineCT64, 64, double, "ct", 256, 3);
-    FFT3D_TWOPASS_STAGED(LineCT64, 64, double, "ct", 384, 2);
-    FFT3D_TWOPASS_STAGED(LineCT64, 64, double, "ct", 128, 3);
-    FFT3D_TWOPASS_STAGED(LineCT64, 64, float, "ct", 128, 6);
-    FFT3D_TWOPASS_STAGED(LineCT64, 64, float, "ct", 256, 3);
-    // 45-point lines as 5 x 9 stages: one plane or y-row per item (complex
-    // double only: a 45-point complex-float row, 360 bytes, cannot be a bulk copy)
     FFT3D_TWOPASS_STAGED(LinePFA45, 45, double, "pfa", 128, 6);
-    // 36-point lines as 4 x 9 stages (tuner candidates; one line per thread wins on B200)
-    FFT3D_TWOPASS_STAGED(LinePFA36, 36, double, "pfa", 128, 8);
-    FFT3D_TWOPASS_STAGED(LinePFA36, 36, float, "pfa", 128, 8);
-    // z pass in shared memory, y and x passes between registers and L2
-    FFT3D_TWOPASS_REGS(36, 36, 36, 3, 128, 3);
-    FFT3D_TWOPASS_REGS(36, 36, 36, 2, 96, 4);
-    FFT3D_TWOPASS_REGS(36, 36, 36, 4, 160, 2);
-    FFT3D_TWOPASS_REGS(36, 36, 36, 2, 96, 3);  // 227 registers: no spills, 9 warps
-    // rows moved by bulk copies: almost no integer work outside the transform
-    FFT3D_TWOPASS_BULK(36, 36, 36, 2, 96, 4);
-    FFT3D_TWOPASS_BULK(36, 36, 36, 3, 128, 3);  // 108 lines on 4 warps: 84% of lanes busy
-    FFT3D_TWOPASS_BULK(36, 36, 36, 4, 160, 2);
-    FFT3D_TWOPASS_BULK(36, 36, 36, 1, 64, 6);
-    FFT3D_TWOPASS_BULK(45, 45, 45, 3, 160, 2);
-    FFT3D_TWOPASS_BULK(45, 45, 45, 5, 256, 1);
-    // two stages per CTA: the next item's copies overlap the current transform
-    FFT3D_TWOPASS_PIPE(36, 36, 36, 2, 96, 2);
-    FFT3D_TWOPASS_PIPE(36, 36, 36, 1, 64, 5);
-    FFT3D_TWOPASS_PIPE(36, 36, 36, 1, 64, 4);
-    FFT3D_TWOPASS_PIPE(36, 36, 36, 4, 160, 1);
-    FFT3D_TWOPASS_PIPE(16, 16, 32, 4, 128, 3);
-    FFT3D_TWOPASS_PIPE(16, 16, 32, 2, 64, 6);
-    // 36^3 and 64^3 with lines split over 4 lanes: about 70 registers a lane
-    FFT3D_TWOPASS_SPLIT(36, 36, 36, double, 2, 288, 2);
-    FFT3D_TWOPASS_SPLIT(36, 36, 36, double, 4, 576, 1);
-    FFT3D_TWOPASS_SPLIT(36, 36, 36, double, 1, 160, 4);
-    FFT3D_TWOPASS_SPLIT(36, 36, 36, float, 4, 576, 1);
-    FFT3D_TWOPASS_SPLIT(36, 36, 36, float, 2, 288, 3);
-    FFT3D_TWOPASS_SPLIT(64, 64, 64, double, 1, 256, 2);
-    FFT3D_TWOPASS_SPLIT(64, 64, 64, double, 2, 512, 1);
-    FFT3D_TWOPASS_SPLIT(64, 64, 64, float, 2, 512, 1);
-    FFT3D_TWOPASS_SPLIT(64, 64, 64, float, 1, 256, 3);
-    // 36^3: 36 lines per plane or row, one thread per line
-    FFT3D_TWOPASS(36, 36, 36, double, 4, 160, 2);
-    FFT3D_TWOPASS(36, 36, 36, double, 2, 96, 4);
-    FFT3D_TWOPASS(36, 36, 36, double, 6, 224, 1);
-    FFT3D_TWOPASS(36, 36, 36, float, 4, 160, 3);
-    FFT3D_TWOPASS(36, 36, 36, float, 6, 224, 2);
-    // 16x16x32 complex double (262 KB): z pass 16*G rows, y and x passes 32*G lines
-    FFT3D_TWOPASS(16, 16, 32, double, 4, 128, 4);
-    FFT3D_TWOPASS(16, 16, 32, double, 8, 256, 2);
-    // 45^3 (45 = 5 x 9) and 64^3 (64 = 8 x 8): beyond any cluster's shared memory
-    FFT3D_TWOPASS(45, 45, 45, double, 3, 160, 2);
-    FFT3D_TWOPASS(45, 45, 45, double, 5, 256, 1);
+    // 45^3 complex float (a 360-byte row cannot be a bulk copy): element copies
     FFT3D_TWOPASS(45, 45, 45, float, 5, 256, 2);
     FFT3D_TWOPASS(45, 45, 45, float, 3, 160, 3);
-    FFT3D_TWOPASS(64, 64, 64, double, 1, 64, 3);
-    FFT3D_TWOPASS(64, 64, 64, double, 2, 128, 1);
+    // 64^3: 64 = 8 x 8 staged lines, one plane or y-row per item
+    FFT3D_TWOPASS_STAGED(LineCT64, 64, double, "ct", 128, 3);
+    FFT3D_TWOPASS_STAGED(LineCT64, 64, double, "ct", 256, 3);
+    FFT3D_TWOPASS_STAGED(LineCT64, 64, float, "ct", 128, 6);
+    FFT3D_TWOPASS_STAGED(LineCT64, 64, float, "ct", 256, 3);
     FFT3D_TWOPASS(64, 64, 64, float, 2, 128, 3);
     FFT3D_TWOPASS(64, 64, 64, float, 4, 256, 1);
 }

@@ -137,9 +137,8 @@ def test_twopass_items(hostcheck, shape, prec, g, nvol, sign):
 
 
 REGS = [((36, 36, 36), 500, 3, 7), ((36, 36, 36), 500, 2, 11), ((36, 36, 36), 500, 4, 3),
-        ((6, 9, 5), 500, 3, 41), ((36, 36, 36), 520, 3, 7), ((36, 36, 36), 520, 2, 5),
-        ((36, 36, 36), 540, 3, 6), ((36, 36, 36), 540, 2, 3), ((45, 45, 45), 520, 3, 3),
-        ((6, 9, 5), 520, 3, 41), ((6, 9, 5), 540, 3, 41)]
+        ((6, 9, 5), 500, 3, 41), ((36, 36, 36), 540, 3, 6), ((36, 36, 36), 540, 2, 3),
+        ((6, 9, 5), 540, 3, 41)]
 # complex float at row pitch 38 (bulk rows): (shape, alg base, G, batch)
 REGS_F = [((36, 36, 36), 540, 3, 7), ((36, 36, 36), 540, 2, 5), ((36, 36, 36), 540, 4, 3)]
 
@@ -166,10 +165,9 @@ def test_twopass_lean_control_complex64(hostcheck, shape, base, g, nvol, sign):
 @pytest.mark.parametrize("sign", [-1, +1])
 def test_twopass_lean_control_variants(hostcheck, shape, base, g, nvol, sign):
     """The lean-control TWOPASS variants: y pass stored straight into the
-    scratch slot and x pass loaded straight from it (alg = 500 + G), y pass in
-    shared memory with row copies and bulk-gathered x pass (520 + G), y pass
-    from registers with bulk-gathered x pass (540 + G); the line maps of
-    pass_y_store_l2 / pass_x_load_l2, in ticket order with the dependency check."""
+    scratch slot and x pass loaded straight from it (alg = 500 + G), or x pass
+    from bulk-gathered rows (540 + G); the line maps of pass_y_store_l2 /
+    pass_x_load_l2, in ticket order with the dependency check."""
     import ctypes
     hostcheck.hostcheck_twopass_violations.restype = ctypes.c_longlong
     hostcheck.hostcheck_twopass_violations()
@@ -181,25 +179,27 @@ def test_twopass_lean_control_variants(hostcheck, shape, base, g, nvol, sign):
     assert oracle.rel_error_per_volume(got, want).max() < C128_TOL
 
 
-SPLIT = [((36, 36, 36), 0, 2, 11), ((36, 36, 36), 0, 1, 3), ((36, 36, 36), 1, 4, 5),
-         ((64, 64, 64), 0, 1, 3), ((64, 64, 64), 1, 2, 2), ((36, 36, 64), 0, 2, 4)]
+STAGED = [(64, 0, 2), (64, 1, 2), (45, 0, 3)]  # (N, precision, batch)
 
 
-@pytest.mark.parametrize("shape,prec,g,nvol", SPLIT,
-                         ids=[f"{t[0]}-c{128 if t[1] == 0 else 64}-g{t[2]}-b{t[3]}" for t in SPLIT])
+@pytest.mark.parametrize("n,prec,nvol", STAGED, ids=[f"{t[0]}-c{128 if t[1] == 0 else 64}" for t in STAGED])
 @pytest.mark.parametrize("sign", [-1, +1])
-def test_twopass_split_lines(hostcheck, shape, prec, g, nvol, sign):
-    """TWOPASS with 36- and 64-point lines spread over 4 lanes (alg = 400 + G):
-    the Good-Thomas (36 = 4 x 9) and Cooley-Tukey (64 = 4 x 16) index maps and
-    the radix-2 lane exchange, in the host form of the kernel's shuffles."""
-    rng = np.random.default_rng(6000 + g + nvol + prec + sum(shape))
+def test_twopass_staged_lines(hostcheck, n, prec, nvol, sign):
+    """The staged TWOPASS kernel (alg = 701): 64-point lines as 8 x 8
+    Cooley-Tukey and 45-point lines as 5 x 9 Good-Thomas stages through shared
+    memory at the kernel's row pitch, rows left in slot order by the z pass."""
+    import ctypes
+    hostcheck.hostcheck_twopass_violations.restype = ctypes.c_longlong
+    hostcheck.hostcheck_twopass_violations()
+    shape = (n, n, n)
+    rng = np.random.default_rng(9000 + n + prec + nvol)
     dt = np.complex128 if prec == 0 else np.complex64
     x = field(rng, (nvol,) + shape, dist="normal", dtype=dt)
-    got = run(hostcheck, x, shape, prec, sign, 400 + g, 1)
+    got = run(hostcheck, x, shape, prec, sign, 701, 1)
+    assert hostcheck.hostcheck_twopass_violations() == 0
     x64 = x.astype(np.complex128)
     want = oracle.fft3d(x64) if sign < 0 else oracle.ifft3d(x64)
-    err = oracle.rel_error_per_volume(got, want).max()
-    assert err < (C128_TOL if prec == 0 else C64_TOL), err
+    assert oracle.rel_error_per_volume(got, want).max() < (C128_TOL if prec == 0 else C64_TOL)
 
 
 LANES = [(2, 2, 11), (2, 4, 5), (1, 4, 3), (3, 4, 7)]  # (G, P, batch)

@@ -6,6 +6,9 @@
 // allocates the per-CTA scratch the two-phase 36^3 kinds need, and captures the
 // ticket reset plus the launch in a CUDA graph.  fft3d_b200_batch_execute
 // replays the graph on the caller's stream: one launch for the whole batch.
+// A batch whose segments are all complex64 runs the complex64 class of the
+// kernel (two CTAs per SM; FFT3D_BATCH_KINDS_C64), any other batch class 0
+// (FFT3D_B200_BATCH_CLASS=0 in the environment forces class 0).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -43,11 +46,38 @@ static const KindInfo kKinds[] = {
 #undef FFT3D_BK_INFO
 };
 
-static const KindInfo *find_kind(int n0, int n1, int n2, int prec, int sign)
+static const KindInfo kKindsC64[] = {
+#define FFT3D_BK_INFO(ID, N0, N1, N2, T, S, VPC, SOLO, BIG)                                   \
+    {ID, N0, N1, N2, sizeof(T) == 8 ? FFT3D_B200_C128 : FFT3D_B200_C64, S, VPC, SOLO, BIG, \
+     (long long)N0 * N1 * N2, kind_stage_bytes<N0, N1, N2, T, VPC, BIG>()},
+    FFT3D_BATCH_KINDS_C64(FFT3D_BK_INFO)
+#undef FFT3D_BK_INFO
+};
+
+static const KindInfo *find_kind(int n0, int n1, int n2, int prec, int sign, int cls = 0)
 {
+    if (cls == 1) {
+        for (const auto &k : kKindsC64)
+            if (k.n0 == n0 && k.n1 == n1 && k.n2 == n2 && k.prec == prec && k.sign == sign) return &k;
+        return nullptr;
+    }
     for (const auto &k : kKinds)
         if (k.n0 == n0 && k.n1 == n1 && k.n2 == n2 && k.prec == prec && k.sign == sign) return &k;
     return nullptr;
+}
+
+// The kernel class a batch runs: its function, threads, shared memory, half.
+struct BatchKernelClass {
+    const void *func;
+    int threads, smem, half;
+};
+
+static BatchKernelClass kernel_class(int cls)
+{
+    if (cls == 1)
+        return {batch_c64_kernel_func(), batch_c64_kernel_threads(), batch_c64_kernel_smem(),
+                batch_c64_kernel_half()};
+    return {batch_kernel_func(), batch_kernel_threads(), batch_kernel_smem(), batch_kernel_half()};
 }
 
 int batch_kind_of(int n0, int n1, int n2, int precision, int sign, int *vpc, int *big,
@@ -78,6 +108,7 @@ struct fft3d_b200_batch {
     long long scratch_per_cta = 0;
     int nitems = 0;
     int grid = 0;
+    int cls = 0;  // kernel class (batch_kernel.cu)
     bool use_graph = false;
     cudaStream_t cap = nullptr;
     cudaGraph_t graph = nullptr;
@@ -129,8 +160,8 @@ static cudaError_t batch_enqueue(fft3d_b200_batch *b, cudaStream_t s)
     int *err = b->d_err;
     void *args[] = {(void *)&items, (void *)&nitems, (void *)&segs,   (void *)&ticket,
                     (void *)&scratch, (void *)&spc,  (void *)&solo, (void *)&err};
-    return cudaLaunchKernel(batch_kernel_func(), dim3(b->grid), dim3(batch_kernel_threads()), args,
-                            (size_t)batch_kernel_smem(), s);
+    const BatchKernelClass kc = kernel_class(b->cls);
+    return cudaLaunchKernel(kc.func, dim3(b->grid), dim3(kc.threads), args, (size_t)kc.smem, s);
 }
 
 // Per-segment strategy on stream s: fork to the branch streams, one tuned plan
@@ -195,10 +226,18 @@ extern "C" int fft3d_b200_batch_create(const fft3d_b200_segment *segs, int nseg,
     std::vector<BatchSeg> dsegs;
     std::vector<unsigned char> solo(BATCH_NKINDS, 0);
     long long scratch_need = 0;
-    for (int k = 0; k < BATCH_NKINDS; ++k) {
-        const KindInfo &ki = kKinds[k];
-        if (ki.stage_bytes > batch_kernel_smem()) return FFT3D_B200_ERR_UNSUPPORTED;
-        solo[k] = (unsigned char)(ki.solo || ki.big || ki.stage_bytes > batch_kernel_half());
+    // every segment complex64: the complex64 class of the kernel
+    int cls = 1;
+    for (int i = 0; i < nseg; ++i)
+        if (segs[i].precision != FFT3D_B200_C64) cls = 0;
+    if (const char *e = getenv("FFT3D_B200_BATCH_CLASS"))
+        if (e[0] == '0') cls = 0;
+    const BatchKernelClass kc = kernel_class(cls);
+    for (const KindInfo &ki : kKinds) {
+        const KindInfo *k = cls == 1 ? find_kind(ki.n0, ki.n1, ki.n2, ki.prec, ki.sign, 1) : &ki;
+        if (!k) continue;
+        if (k->stage_bytes > kc.smem) return FFT3D_B200_ERR_UNSUPPORTED;
+        solo[k->id] = (unsigned char)(k->solo || k->big || k->stage_bytes > kc.half);
     }
     for (int i = 0; i < nseg; ++i) {
         const fft3d_b200_segment &s = segs[i];
@@ -207,7 +246,7 @@ extern "C" int fft3d_b200_batch_create(const fft3d_b200_segment *segs, int nseg,
             return FFT3D_B200_ERR_INVALID;
         if (s.precision != FFT3D_B200_C128 && s.precision != FFT3D_B200_C64)
             return FFT3D_B200_ERR_INVALID;
-        const KindInfo *k = find_kind(s.n0, s.n1, s.n2, s.precision, s.direction);
+        const KindInfo *k = find_kind(s.n0, s.n1, s.n2, s.precision, s.direction, cls);
         if (!k) return FFT3D_B200_ERR_UNSUPPORTED;
         const size_t eb = (size_t)element_bytes(s.precision);
         const size_t bytes = (size_t)s.batch * (size_t)k->vol_elems * eb;
@@ -238,8 +277,8 @@ extern "C" int fft3d_b200_batch_create(const fft3d_b200_segment *segs, int nseg,
     }
     if (items.size() > 0x7fffffff) return FFT3D_B200_ERR_INVALID;
     // largest first: big items start early, small ones fill the tail
-    std::stable_sort(items.begin(), items.end(), [](const BatchItem &a, const BatchItem &b) {
-        const KindInfo &ka = kKinds[a.kind], &kb = kKinds[b.kind];
+    std::stable_sort(items.begin(), items.end(), [&](const BatchItem &a, const BatchItem &b) {
+        const KindInfo &ka = kKinds[a.kind], &kb = kKinds[b.kind];  // extents and precision
         const long long ca = (long long)a.nv * ka.vol_elems * (ka.prec == FFT3D_B200_C128 ? 16 : 8);
         const long long cb = (long long)b.nv * kb.vol_elems * (kb.prec == FFT3D_B200_C128 ? 16 : 8);
         return ca > cb;
@@ -258,6 +297,7 @@ extern "C" int fft3d_b200_batch_create(const fft3d_b200_segment *segs, int nseg,
     b->device = device;
     b->segs.assign(segs, segs + nseg);
     b->nitems = (int)items.size();
+    b->cls = cls;
     auto fail = [&](int code) {
         const cudaError_t ce = cudaGetLastError();
         if (getenv("FFT3D_B200_DEBUG"))
@@ -266,14 +306,11 @@ extern "C" int fft3d_b200_batch_create(const fft3d_b200_segment *segs, int nseg,
         if (prev >= 0) cudaSetDevice(prev);
         return code;
     };
-    if (cudaFuncSetAttribute(batch_kernel_func(), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             batch_kernel_smem()) != cudaSuccess)
+    if (cudaFuncSetAttribute(kc.func, cudaFuncAttributeMaxDynamicSharedMemorySize, kc.smem) != cudaSuccess)
         return fail(FFT3D_B200_ERR_CUDA);
     int occ = 0, sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_kernel_func(),
-                                                      batch_kernel_threads(),
-                                                      (size_t)batch_kernel_smem()) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kc.func, kc.threads, (size_t)kc.smem) != cudaSuccess ||
         occ < 1)
         return fail(FFT3D_B200_ERR_UNSUPPORTED);
     b->grid = std::max(1, std::min(occ * sms, std::max(1, b->nitems)));
@@ -370,8 +407,9 @@ extern "C" int fft3d_b200_batch_create(const fft3d_b200_segment *segs, int nseg,
                  "batch: %d segments, one tuned plan per segment on %zu parallel branches, %s",
                  nseg, b->branch.size(), b->use_graph ? "CUDA graph" : "direct launches");
     } else {
-        snprintf(buf, sizeof buf, "batch: %d segments, %d items, grid %d x %d threads, %s%s", nseg,
-                 b->nitems, b->grid, batch_kernel_threads(), b->use_graph ? "CUDA graph" : "direct launch",
+        snprintf(buf, sizeof buf, "batch: %d segments, %d items, grid %d x %d threads (%s kernel), %s%s",
+                 nseg, b->nitems, b->grid, kernel_class(b->cls).threads,
+                 b->cls == 1 ? "complex64" : "all-kinds", b->use_graph ? "CUDA graph" : "direct launch",
                  b->d_scratch ? ", two-phase scratch" : "");
     }
     b->describe = buf;

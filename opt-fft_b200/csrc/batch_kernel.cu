@@ -9,6 +9,13 @@
 // with cp.async while the previous one is transformed out of the other half;
 // larger items (24^3 and 16x16x32 complex double) use all of it.
 //
+// Two classes of the kernel share this code: class 0 carries every kind (320
+// threads, one CTA per SM, 227 KB of shared memory); class 1 carries the
+// complex64 kinds only (batch_kinds.h FFT3D_BATCH_KINDS_C64), whose lines need
+// fewer registers, as two 256-thread CTAs per SM with half the shared memory
+// each, items re-sized to match -- twice the resident warps for an all-complex64
+// batch.
+//
 // 36^3 does not fit one SM.  In this kernel a single CTA transforms it in two
 // phases through a per-CTA scratch volume in global memory: x-slabs (z and y
 // passes) are written to scratch, then y-slabs are read back for the x pass and
@@ -22,18 +29,30 @@
 
 namespace fft3d {
 
-constexpr int BATCH_THREADS = 320;
-// 227 KB is the per-CTA maximum on sm_100a, static shared memory included; keep
-// 128 bytes for this kernel's static variables.
-constexpr int BATCH_SMEM = 232448 - 128;
-constexpr int BATCH_HALF = (BATCH_SMEM / 2) / 128 * 128;
+template <int CLS>
+struct BatchClass;
+template <>
+struct BatchClass<0> {
+    static constexpr int NT = 320, MINB = 1;
+    // 227 KB is the per-CTA maximum on sm_100a, static shared memory included;
+    // keep 128 bytes for this kernel's static variables.
+    static constexpr int SMEM = 232448 - 128;
+    static constexpr int HALF = (SMEM / 2) / 128 * 128;
+};
+template <>
+struct BatchClass<1> {
+    static constexpr int NT = 256, MINB = 2;
+    // two CTAs in the SM's 228 KB, each with its 1 KB reserve and static variables
+    static constexpr int SMEM = (233472 - 2 * 1024) / 2 - 256;
+    static constexpr int HALF = (SMEM / 2) / 128 * 128;
+};
 
 // cp.async copy of nel elements into the layout of G (row = g / N2).
-template <class G>
+template <int NT, class G>
 __device__ __forceinline__ void batch_load(cx<typename G::T> *sm, const cx<typename G::T> *gin,
                                            int nel)
 {
-    for (int g = threadIdx.x; g < nel; g += BATCH_THREADS) {
+    for (int g = threadIdx.x; g < nel; g += NT) {
         const int vol = g / G::V;
         const int rem = g - vol * G::V;
         cx<typename G::T> *dst = sm + G::off(vol * G::ROWS + rem / G::N2, rem % G::N2);
@@ -43,46 +62,46 @@ __device__ __forceinline__ void batch_load(cx<typename G::T> *sm, const cx<typen
     cp_async_commit();
 }
 
-template <class G, int S>
+template <int NT, class G, int S>
 __device__ __forceinline__ void batch_passes(cx<typename G::T> *sm, int nv,
                                              cx<typename G::T> *gout, typename G::T scale)
 {
     const int tid = threadIdx.x;
-    for (int r = tid; r < nv * G::ROWS; r += BATCH_THREADS) pass_z<G, S, ALG_DEFAULT>(sm, r);
+    for (int r = tid; r < nv * G::ROWS; r += NT) pass_z<G, S, ALG_DEFAULT>(sm, r);
     __syncthreads();
-    for (int l = tid; l < nv * G::N0 * G::N2; l += BATCH_THREADS) pass_y<G, S, ALG_DEFAULT>(sm, l);
+    for (int l = tid; l < nv * G::N0 * G::N2; l += NT) pass_y<G, S, ALG_DEFAULT>(sm, l);
     __syncthreads();
-    for (int l = tid; l < nv * G::N1 * G::N2; l += BATCH_THREADS)
-        pass_x_out<G, S, ALG_DEFAULT>(sm, l, gout, scale);
+    for (int l = tid; l < nv * G::N1 * G::N2; l += NT) pass_x_out<G, S, ALG_DEFAULT>(sm, l, gout, scale);
 }
 
 // ---------------------------------------------------------------- two-phase large cube
 
 // One L^3 volume by one CTA: NS x-slabs of PL planes, then NS y-slabs of PL rows.
-template <int L, typename T, int S, int PL>
+template <int NT, int L, typename T, int S, int PL>
 __device__ __forceinline__ void big_cube(cx<T> *sm, const cx<T> *gin, cx<T> *gout, cx<T> *scratch, T scale)
 {
     constexpr int NS = L / PL;
+    static_assert(NS * PL == L, "slabs of PL planes");
     using XG = Geom<PL, L, L, T>;  // x-slab: PL planes of L x L
     using YG = Geom<L, PL, L, T>;  // y-slab: all x, PL rows of y
     const int tid = threadIdx.x;
     for (int s = 0; s < NS; ++s) {
-        batch_load<XG>(sm, gin + (long long)s * PL * L * L, PL * L * L);
+        batch_load<NT, XG>(sm, gin + (long long)s * PL * L * L, PL * L * L);
         cp_async_wait<0>();
         __syncthreads();
-        for (int r = tid; r < PL * L; r += BATCH_THREADS) pass_z<XG, S, ALG_DEFAULT>(sm, r);
+        for (int r = tid; r < PL * L; r += NT) pass_z<XG, S, ALG_DEFAULT>(sm, r);
         __syncthreads();
-        for (int l = tid; l < PL * L; l += BATCH_THREADS) pass_y<XG, S, ALG_DEFAULT>(sm, l);
+        for (int l = tid; l < PL * L; l += NT) pass_y<XG, S, ALG_DEFAULT>(sm, l);
         __syncthreads();
         cx<T> *dst = scratch + (long long)s * PL * L * L;
-        for (int g = tid; g < PL * L * L; g += BATCH_THREADS) dst[g] = sm[XG::off(g / L, g % L)];
+        for (int g = tid; g < PL * L * L; g += NT) dst[g] = sm[XG::off(g / L, g % L)];
         __syncthreads();
     }
     __threadfence();
     __syncthreads();
     for (int s = 0; s < NS; ++s) {
         // rows (x, y - s*PL) of the y-slab; the source rows are L*L apart in scratch
-        for (int g = tid; g < L * PL * L; g += BATCH_THREADS) {
+        for (int g = tid; g < L * PL * L; g += NT) {
             const int z = g % L;
             const int row = g / L;  // x * PL + yl
             const int x = row / PL, yl = row % PL;
@@ -94,41 +113,34 @@ __device__ __forceinline__ void big_cube(cx<T> *sm, const cx<T> *gin, cx<T> *gou
         cp_async_commit();
         cp_async_wait<0>();
         __syncthreads();
-        for (int l = tid; l < PL * L; l += BATCH_THREADS) pass_x_slab<YG, S, L>(sm, l, gout, s * PL, scale);
+        for (int l = tid; l < PL * L; l += NT) pass_x_slab<YG, S, L>(sm, l, gout, s * PL, scale);
         __syncthreads();
     }
 }
 
 // ---------------------------------------------------------------- dispatch
 
-template <class G, int S>
+template <int NT, class G, int S>
 __device__ __forceinline__ void run_kind_small(unsigned char *region, const BatchItem &it,
                                                const BatchSeg &sg)
 {
     using T = typename G::T;
-    const cx<T> *gin = reinterpret_cast<const cx<T> *>(sg.in) + it.v0 * G::V;
     cx<T> *gout = reinterpret_cast<cx<T> *>(sg.out) + it.v0 * G::V;
-    batch_passes<G, S>(reinterpret_cast<cx<T> *>(region), it.nv, gout, (T)sg.scale);
-    (void)gin;
+    batch_passes<NT, G, S>(reinterpret_cast<cx<T> *>(region), it.nv, gout, (T)sg.scale);
 }
 
-template <class G>
-__device__ __forceinline__ void load_kind(unsigned char *region, const BatchItem &it,
-                                          const BatchSeg &sg)
-{
-    using T = typename G::T;
-    const cx<T> *gin = reinterpret_cast<const cx<T> *>(sg.in) + it.v0 * G::V;
-    batch_load<G>(reinterpret_cast<cx<T> *>(region), gin, it.nv * G::V);
-}
-
-template <int N0, int N1, int N2, typename T, int BIG>
+template <int NT, int N0, int N1, int N2, typename T, int BIG>
 __device__ __forceinline__ void load_kind_any(unsigned char *region, const BatchItem &it,
                                               const BatchSeg &sg)
 {
-    if constexpr (BIG == 0) load_kind<Geom<N0, N1, N2, T>>(region, it, sg);
+    if constexpr (BIG == 0) {
+        using G = Geom<N0, N1, N2, T>;
+        const cx<T> *gin = reinterpret_cast<const cx<T> *>(sg.in) + it.v0 * G::V;
+        batch_load<NT, G>(reinterpret_cast<cx<T> *>(region), gin, it.nv * G::V);
+    }
 }
 
-template <int N0, int N1, int N2, typename T, int S, int BIG>
+template <int NT, int N0, int N1, int N2, typename T, int S, int BIG>
 __device__ __forceinline__ void run_kind_any(unsigned char *region, const BatchItem &it,
                                              const BatchSeg &sg, unsigned char *scratch)
 {
@@ -136,42 +148,62 @@ __device__ __forceinline__ void run_kind_any(unsigned char *region, const BatchI
         constexpr long long V = (long long)N0 * N1 * N2;
         const cx<T> *gin = reinterpret_cast<const cx<T> *>(sg.in) + it.v0 * V;
         cx<T> *gout = reinterpret_cast<cx<T> *>(sg.out) + it.v0 * V;
-        big_cube<N0, T, S, BIG>(reinterpret_cast<cx<T> *>(region), gin, gout,
-                                reinterpret_cast<cx<T> *>(scratch), (T)sg.scale);
+        big_cube<NT, N0, T, S, BIG>(reinterpret_cast<cx<T> *>(region), gin, gout,
+                                    reinterpret_cast<cx<T> *>(scratch), (T)sg.scale);
     } else {
-        run_kind_small<Geom<N0, N1, N2, T>, S>(region, it, sg);
+        run_kind_small<NT, Geom<N0, N1, N2, T>, S>(region, it, sg);
     }
 }
 
 // Issue the loads of an item (two-phase cubes load inside run_item).
+template <int CLS>
 __device__ __forceinline__ void issue_item_load(unsigned char *region, const BatchItem &it, const BatchSeg &sg)
 {
-    switch (it.kind) {
+    constexpr int NT = BatchClass<CLS>::NT;
 #define FFT3D_BK_LOAD(ID, N0, N1, N2, T, S, VPC, SOLO, BIG) \
-    case ID: load_kind_any<N0, N1, N2, T, BIG>(region, it, sg); break;
-        FFT3D_BATCH_KINDS(FFT3D_BK_LOAD)
+    case ID: load_kind_any<NT, N0, N1, N2, T, BIG>(region, it, sg); break;
+    if constexpr (CLS == 0) {
+        switch (it.kind) {
+            FFT3D_BATCH_KINDS(FFT3D_BK_LOAD)
+        default: break;
+        }
+    } else {
+        switch (it.kind) {
+            FFT3D_BATCH_KINDS_C64(FFT3D_BK_LOAD)
+        default: break;
+        }
+    }
 #undef FFT3D_BK_LOAD
-    default: break;
-    }
 }
 
+template <int CLS>
 __device__ __forceinline__ void run_item(unsigned char *region, const BatchItem &it, const BatchSeg &sg,
-                         unsigned char *scratch_bytes)
+                                         unsigned char *scratch_bytes)
 {
-    switch (it.kind) {
+    constexpr int NT = BatchClass<CLS>::NT;
 #define FFT3D_BK_RUN(ID, N0, N1, N2, T, S, VPC, SOLO, BIG) \
-    case ID: run_kind_any<N0, N1, N2, T, S, BIG>(region, it, sg, scratch_bytes); break;
-        FFT3D_BATCH_KINDS(FFT3D_BK_RUN)
-#undef FFT3D_BK_RUN
-    default: break;
+    case ID: run_kind_any<NT, N0, N1, N2, T, S, BIG>(region, it, sg, scratch_bytes); break;
+    if constexpr (CLS == 0) {
+        switch (it.kind) {
+            FFT3D_BATCH_KINDS(FFT3D_BK_RUN)
+        default: break;
+        }
+    } else {
+        switch (it.kind) {
+            FFT3D_BATCH_KINDS_C64(FFT3D_BK_RUN)
+        default: break;
+        }
     }
+#undef FFT3D_BK_RUN
 }
 
-__global__ void __launch_bounds__(BATCH_THREADS, 1)
+template <int CLS>
+__global__ void __launch_bounds__(BatchClass<CLS>::NT, BatchClass<CLS>::MINB)
     k_batch(const BatchItem *__restrict__ items, int nitems, const BatchSeg *__restrict__ segs,
             unsigned int *ticket, unsigned char *scratch, long long scratch_per_cta,
             const unsigned char *__restrict__ solo_of_kind, int *err)
 {
+    constexpr int HALF = BatchClass<CLS>::HALF;
     extern __shared__ __align__(128) unsigned char smraw[];
     __shared__ int s_next;
     (void)err;
@@ -184,7 +216,7 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1)
     int off = 0;  // byte offset of the current item's region
     if (cur < nitems) {
         const BatchItem it = items[cur];
-        issue_item_load(smraw, it, segs[it.seg]);
+        issue_item_load<CLS>(smraw, it, segs[it.seg]);
     }
     while (cur < nitems) {
         const BatchItem it = items[cur];
@@ -199,19 +231,19 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1)
             const BatchItem nt = items[next];
             if (!solo_of_kind[nt.kind]) {
                 pre = true;
-                noff = off == 0 ? BATCH_HALF : 0;
-                issue_item_load(smraw + noff, nt, segs[nt.seg]);
+                noff = off == 0 ? HALF : 0;
+                issue_item_load<CLS>(smraw + noff, nt, segs[nt.seg]);
             }
         }
         if (pre) cp_async_wait<1>();
         else cp_async_wait<0>();
         __syncthreads();
-        run_item(smraw + off, it, segs[it.seg], my_scratch);
+        run_item<CLS>(smraw + off, it, segs[it.seg], my_scratch);
         __syncthreads();
         if (!pre && next < nitems) {
             const BatchItem nt = items[next];
             noff = 0;
-            issue_item_load(smraw, nt, segs[nt.seg]);
+            issue_item_load<CLS>(smraw, nt, segs[nt.seg]);
         }
         cur = next;
         off = noff;
@@ -219,9 +251,13 @@ __global__ void __launch_bounds__(BATCH_THREADS, 1)
     cp_async_wait<0>();
 }
 
-const void *batch_kernel_func() { return (const void *)&k_batch; }
-int batch_kernel_threads() { return BATCH_THREADS; }
-int batch_kernel_smem() { return BATCH_SMEM; }
-int batch_kernel_half() { return BATCH_HALF; }
+const void *batch_kernel_func() { return (const void *)&k_batch<0>; }
+int batch_kernel_threads() { return BatchClass<0>::NT; }
+int batch_kernel_smem() { return BatchClass<0>::SMEM; }
+int batch_kernel_half() { return BatchClass<0>::HALF; }
+const void *batch_c64_kernel_func() { return (const void *)&k_batch<1>; }
+int batch_c64_kernel_threads() { return BatchClass<1>::NT; }
+int batch_c64_kernel_smem() { return BatchClass<1>::SMEM; }
+int batch_c64_kernel_half() { return BatchClass<1>::HALF; }
 
 }  // namespace fft3d

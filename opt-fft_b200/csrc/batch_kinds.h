@@ -68,6 +68,29 @@ struct BatchSeg {
 
 constexpr int BATCH_NKINDS = 36;
 
+// The complex64 kinds for the class-1 kernel (two CTAs per SM, half the shared
+// memory each): the same ids, volumes per item re-sized for a 57 KB half, and
+// 24^3 (115 KB a volume) through the two-phase route as well.
+#define FFT3D_BATCH_KINDS_C64(X)                     \
+    X(18, 6, 6, 6, float, -1, 28, 0, 0)              \
+    X(19, 6, 6, 6, float, +1, 28, 0, 0)              \
+    X(20, 8, 8, 8, float, -1, 12, 0, 0)              \
+    X(21, 8, 8, 8, float, +1, 12, 0, 0)              \
+    X(22, 12, 12, 12, float, -1, 3, 0, 0)            \
+    X(23, 12, 12, 12, float, +1, 3, 0, 0)            \
+    X(24, 16, 16, 16, float, -1, 1, 0, 0)            \
+    X(25, 16, 16, 16, float, +1, 1, 0, 0)            \
+    X(26, 17, 17, 17, float, -1, 1, 0, 0)            \
+    X(27, 17, 17, 17, float, +1, 1, 0, 0)            \
+    X(28, 24, 24, 24, float, -1, 1, 1, 12)           \
+    X(29, 24, 24, 24, float, +1, 1, 1, 12)           \
+    X(30, 36, 36, 36, float, -1, 1, 1, 9)            \
+    X(31, 36, 36, 36, float, +1, 1, 1, 9)            \
+    X(32, 8, 8, 16, float, -1, 7, 0, 0)              \
+    X(33, 8, 8, 16, float, +1, 7, 0, 0)              \
+    X(34, 16, 16, 32, float, -1, 1, 1, 0)            \
+    X(35, 16, 16, 32, float, +1, 1, 1, 0)
+
 // Kind lookup for the host side (batch.cu): returns the kind id or -1, and the
 // kind's volumes per item, two-phase flag, volume size, and whether its items
 // need all of shared memory.
@@ -78,5 +101,10 @@ const void *batch_kernel_func();
 int batch_kernel_threads();
 int batch_kernel_smem();
 int batch_kernel_half();
+// the complex64 class (FFT3D_BATCH_KINDS_C64)
+const void *batch_c64_kernel_func();
+int batch_c64_kernel_threads();
+int batch_c64_kernel_smem();
+int batch_c64_kernel_half();
 
 }  // namespace fft3d

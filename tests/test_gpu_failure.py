@@ -20,15 +20,21 @@ pytestmark = pytest.mark.gpu
 import fft3d_b200 as fb  # noqa: E402
 
 
-@pytest.mark.parametrize("variant", ["twopass 36x36x36 double g2 bulk nt96 minb4",
-                                     "twopass 36x36x36 double g2 nt96 minb4"])
-def test_dependency_wait_runs_out_and_plan_recovers(variant):
-    shape, b = (36, 36, 36), 50
+# the three TWOPASS item loops: lean control (bulk rows, L2 policies), lines
+# over lanes, and the plain loop
+CASES = [((36, 36, 36), fb.C128, "twopass 36x36x36 double g2 bulkqh nt96 minb4"),
+         ((36, 36, 36), fb.C128, "twopass 36x36x36 double g2 lanes4 nt288 minb3"),
+         ((45, 45, 45), fb.C64, "twopass 45x45x45 float g3 nt160 minb3")]
+
+
+@pytest.mark.parametrize("shape,prec,variant", CASES, ids=[c[2] for c in CASES])
+def test_dependency_wait_runs_out_and_plan_recovers(shape, prec, variant):
+    b = 50
     rng = np.random.default_rng(5)
-    x = field(rng, (b,) + shape)
+    x = field(rng, (b,) + shape, dtype=np.complex128 if prec == fb.C128 else np.complex64)
     xi = torch.from_numpy(x).cuda()
     xo = torch.zeros_like(xi)
-    plan = fb.Plan(shape, b, fb.FORWARD, fb.C128, variant=variant)
+    plan = fb.Plan(shape, b, fb.FORWARD, prec, variant=variant)
     lib = fb.lib()
     assert lib.fft3d_b200_debug_stall_next_execute(plan.handle) == fb.OK
     t0 = time.time()
@@ -40,8 +46,9 @@ def test_dependency_wait_runs_out_and_plan_recovers(variant):
     # the context and the plan are still usable: the next execute is exact
     plan.execute(xi.data_ptr(), xo.data_ptr())
     assert lib.fft3d_b200_plan_check(plan.handle) == fb.OK
-    got = xo.cpu().numpy()
-    assert oracle.rel_error_per_volume(got, oracle.fft3d(x)).max() < 1e-13
+    got = xo.cpu().numpy().astype(np.complex128)
+    tol = 1e-13 if prec == fb.C128 else 1e-6
+    assert oracle.rel_error_per_volume(got, oracle.fft3d(x.astype(np.complex128))).max() < tol
     plan.close()
 
 

@@ -92,11 +92,13 @@ def test_cluster_data_movement(hostcheck, prec, c, sign):
     assert err < (C128_TOL if prec == 0 else C64_TOL), err
 
 
-@pytest.mark.parametrize("prec,pl", [(0, 9), (1, 12)])
+@pytest.mark.parametrize("n,prec,pl", [(36, 0, 9), (36, 1, 12), (36, 1, 9), (24, 1, 12)])
 @pytest.mark.parametrize("sign", [-1, +1])
-def test_two_phase_cube(hostcheck, prec, pl, sign):
-    """The batch kernel's two-phase 36^3 route through scratch (alg = 200 + slab)."""
-    shape = (36, 36, 36)
+def test_two_phase_cube(hostcheck, n, prec, pl, sign):
+    """The batch kernel's two-phase route through scratch (alg = 200 + slab
+    planes): 36^3 in both kernel classes' slabs, 24^3 complex64 in the
+    complex64 class."""
+    shape = (n, n, n)
     rng = np.random.default_rng(4000 + pl)
     dt = np.complex128 if prec == 0 else np.complex64
     x = field(rng, (2,) + shape, dist="normal", dtype=dt)

@@ -307,3 +307,36 @@ def test_linearity_full_batch_c64():
     fy, _ = run_plan(p, y)
     fxy, _ = run_plan(p, (x + y).astype(np.complex64))
     assert oracle.rel_error(fxy.astype(np.complex128), (fx + fy).astype(np.complex128)) < 1e-6
+
+
+@pytest.mark.parametrize("shape,batch", [((8, 8, 8), (1 << 21) + 3), ((17, 17, 17), 230_003)])
+def test_batches_past_32_bit_offsets(shape, batch):
+    """A batch whose element offsets pass 2^31 and byte offsets 2^34 (17 GB a
+    buffer): the first, a middle and the last volumes against the oracle, and
+    the forward -> inverse round trip of every volume on the device."""
+    vol = int(np.prod(shape))
+    assert batch * vol > (1 << 31)
+    g = torch.Generator(device="cuda").manual_seed(77)
+    x = torch.empty((batch,) + shape, dtype=torch.complex128, device="cuda")
+    x.real.uniform_(-1.0, 1.0, generator=g)
+    x.imag.uniform_(-1.0, 1.0, generator=g)
+    y = torch.empty_like(x)
+    f = fb.Plan(shape, batch, fb.FORWARD, fb.C128)
+    f.execute(x.data_ptr(), y.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    f.check()
+    for k in (0, batch // 2 + 1, batch - 1):
+        xs = x[k:k + 1].cpu().numpy()
+        assert oracle.rel_error(y[k:k + 1].cpu().numpy(), oracle.fft3d(xs)) < C128_TOL, k
+    f.close()
+    i = fb.Plan(shape, batch, fb.BACKWARD, fb.C128)
+    back = torch.empty_like(x)
+    i.execute(y.data_ptr(), back.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    i.check()
+    del y
+    # per-volume relative L2 of the round trip, every volume, on the device
+    d = (back - x).reshape(batch, -1).abs().pow(2).sum(1).sqrt()
+    n = x.reshape(batch, -1).abs().pow(2).sum(1).sqrt()
+    assert float((d / n).max()) < C128_TOL
+    i.close()

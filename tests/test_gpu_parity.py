@@ -309,10 +309,10 @@ def test_linearity_full_batch_c64():
     assert oracle.rel_error(fxy.astype(np.complex128), (fx + fy).astype(np.complex128)) < 1e-6
 
 
-@pytest.mark.parametrize("shape,batch", [((8, 8, 8), (1 << 22) + 3), ((36, 36, 36), 4000)])
+@pytest.mark.parametrize("shape,batch", [((8, 8, 8), (1 << 22) + 3), ((36, 36, 36), 6000)])
 def test_large_batches_64_bit_offsets(shape, batch):
     """Maximum sizes: 2^22 + 3 volumes of 8^3 put element offsets past 2^31
-    (34 GB a buffer, about 100 GB on the device in all); 4000 volumes of 36^3
+    (34 GB a buffer, about 100 GB on the device in all); 6000 volumes of 36^3
     put the TWOPASS kernel's byte offsets past 2^32.  The first, a middle and
     the last volumes against the oracle, and the forward -> inverse round trip
     of every volume on the device."""

@@ -327,6 +327,30 @@ def time_e2e(fb, torch, wl, steps, warmup, dist=None):
     return dt, wl.bytes, wl.bytes
 
 
+def pcie_floor(torch, wl, reps=5):
+    """Seconds per step of the e2e transfers alone: the step's input uploaded
+    and its output downloaded at the same time (page-locked buffers, two
+    streams), no transform -- the bound the e2e step approaches."""
+    pin_in = torch.from_numpy(wl.host).pin_memory()
+    pin_out = torch.empty_like(pin_in).pin_memory()
+    d_in = torch.empty(pin_in.shape, dtype=pin_in.dtype, device="cuda")
+    d_out = torch.empty_like(d_in)
+    up, down = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def once():
+        with torch.cuda.stream(up):
+            d_in.copy_(pin_in, non_blocking=True)
+        with torch.cuda.stream(down):
+            pin_out.copy_(d_out, non_blocking=True)
+        up.synchronize()
+        down.synchronize()
+    once()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        once()
+    return (time.perf_counter() - t0) / reps
+
+
 # ------------------------------------------------------------------ uneven mixed batch
 
 MIX = [((6, 6, 6), 8192), ((8, 8, 8), 4096), ((12, 12, 12), 2048), ((16, 16, 16), 1024),
@@ -907,6 +931,11 @@ def main():
         e2e = {"value": world * wl.batch / e2e_s, "unit": "volumes/s", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h,
                "path": "fft3d_b200_execute_host_chain, page-locked host buffers"}
+        floor_s = pcie_floor(torch, wl)
+        e2e["pcie_floor"] = {"value": wl.batch / floor_s, "unit": "volumes/s",
+                             "ms_per_step": floor_s * 1e3,
+                             "what": "the same bytes uploaded and downloaded concurrently, no transform"}
+        e2e["frac_of_pcie_floor"] = (wl.batch / e2e_s) / (wl.batch / floor_s)
 
     workloads = {}
     per_l = {a.workload: [value, roofline["frac"], roofline["kernel"]]}

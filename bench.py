@@ -931,11 +931,12 @@ def main():
         e2e = {"value": world * wl.batch / e2e_s, "unit": "volumes/s", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h,
                "path": "fft3d_b200_execute_host_chain, page-locked host buffers"}
-        floor_s = pcie_floor(torch, wl)
-        e2e["pcie_floor"] = {"value": wl.batch / floor_s, "unit": "volumes/s",
-                             "ms_per_step": floor_s * 1e3,
-                             "what": "the same bytes uploaded and downloaded concurrently, no transform"}
-        e2e["frac_of_pcie_floor"] = (wl.batch / e2e_s) / (wl.batch / floor_s)
+        if world == 1:
+            floor_s = pcie_floor(torch, wl)
+            e2e["pcie_floor"] = {"value": wl.batch / floor_s, "unit": "volumes/s",
+                                 "ms_per_step": floor_s * 1e3,
+                                 "what": "the same bytes uploaded and downloaded concurrently, no transform"}
+            e2e["frac_of_pcie_floor"] = e2e_s and floor_s / e2e_s
 
     workloads = {}
     per_l = {a.workload: [value, roofline["frac"], roofline["kernel"]]}

@@ -83,7 +83,10 @@ int fft3d_b200_execute(fft3d_b200_plan *plan, const void *d_in, void *d_out, voi
 
 /* Transform host data: copies in, transforms, copies out, and returns when `out`
  * holds the result.  Page-locked buffers are transferred directly; pageable ones
- * through the plan's pinned staging, in overlapped chunks. */
+ * through the plan's pinned staging, in overlapped chunks.  Chunks are whole
+ * volumes, at most about 1/8 of the batch (4..64 MB), with smaller chunks first
+ * and last; FFT3D_B200_HOST_CHUNK_MB=<n> in the environment (read when a plan
+ * first transfers host data) sets the largest chunk instead. */
 int fft3d_b200_execute_host(fft3d_b200_plan *plan, const void *h_in, void *h_out);
 
 /* Run plans[0], plans[1], ... back to back on the device between ONE host-to-device

@@ -775,9 +775,13 @@ static int ensure_staging(fft3d_b200_plan *p)
         free_staging(p);
         return FFT3D_B200_ERR_NOMEM;
     }
-    // about 8 chunks per batch (4..64 MB, whole volumes): on PCIe Gen5 x16 a
-    // 161 MB round trip pipelines in 3.66 ms with 8 chunks and 4.24 ms with 20
-    const size_t target = std::min<size_t>((size_t)64 << 20, std::max<size_t>((size_t)4 << 20, p->bytes / 8));
+    // the largest chunk: about 1/8 of the batch (4..64 MB, whole volumes), or
+    // FFT3D_B200_HOST_CHUNK_MB; run_host_chain ramps the first and last chunks
+    size_t target = std::min<size_t>((size_t)64 << 20, std::max<size_t>((size_t)4 << 20, p->bytes / 8));
+    if (const char *e = getenv("FFT3D_B200_HOST_CHUNK_MB")) {
+        const long mb = strtol(e, nullptr, 10);
+        if (mb >= 1 && mb <= 4096) target = (size_t)mb << 20;
+    }
     size_t chunk = std::max(vb, (target + vb - 1) / vb * vb);
     chunk = std::min(chunk, p->bytes);
     p->pin_bytes = chunk;

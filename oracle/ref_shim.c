@@ -351,7 +351,11 @@ ref_ctx *ref_open(int backend, int n0, int n1, int n2, long batch, int precision
         snprintf(c->name, sizeof c->name, "FFTW 3.3.10 plan_many_dft %s%s, %s", precision ? "fftwf " : "",
                  effort_name(effort),
                  backend == REF_FFTW ? "one plan per thread slice" : "fftw_plan_with_nthreads");
-    if (pool_start(c)) goto fail;
+    if (pool_start(c)) {
+        /* workers already started wait on this context's barrier: it is left
+           allocated (a leak on this error path only) rather than freed under them */
+        return NULL;
+    }
     return c;
 fail:
     free(c);  /* plans leak on this error path only; the baseline then reports it */

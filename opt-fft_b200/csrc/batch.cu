@@ -226,6 +226,7 @@ extern "C" int fft3d_b200_batch_create(const fft3d_b200_segment *segs, int nseg,
     std::vector<BatchSeg> dsegs;
     std::vector<unsigned char> solo(BATCH_NKINDS, 0);
     long long scratch_need = 0;
+    bool persistent_ok = true;  // every segment has a kind of the persistent kernel
     // every segment complex64: the complex64 class of the kernel
     int cls = 1;
     for (int i = 0; i < nseg; ++i)
@@ -246,15 +247,22 @@ extern "C" int fft3d_b200_batch_create(const fft3d_b200_segment *segs, int nseg,
             return FFT3D_B200_ERR_INVALID;
         if (s.precision != FFT3D_B200_C128 && s.precision != FFT3D_B200_C64)
             return FFT3D_B200_ERR_INVALID;
-        const KindInfo *k = find_kind(s.n0, s.n1, s.n2, s.precision, s.direction, cls);
-        if (!k) return FFT3D_B200_ERR_UNSUPPORTED;
         const size_t eb = (size_t)element_bytes(s.precision);
-        const size_t bytes = (size_t)s.batch * (size_t)k->vol_elems * eb;
+        const size_t bytes = (size_t)s.batch * (size_t)s.n0 * (size_t)s.n1 * (size_t)s.n2 * eb;
         if (s.batch > 0) {
             if (!s.in || !s.out) return FFT3D_B200_ERR_INVALID;
             if (((uintptr_t)s.in % eb) || ((uintptr_t)s.out % eb)) return FFT3D_B200_ERR_ALIGN;
             const char *a = (const char *)s.in, *o = (const char *)s.out;
             if (a < o + bytes && o < a + bytes) return FFT3D_B200_ERR_OVERLAP;
+        }
+        const KindInfo *k = find_kind(s.n0, s.n1, s.n2, s.precision, s.direction, cls);
+        if (!k) {
+            // no persistent-kernel kind for this extent: the batch runs as one
+            // tuned plan per segment (if the extent has a plan at all)
+            if ((flags & FFT3D_B200_BATCH_PERSISTENT) || !fft3d_b200_supports(s.n0, s.n1, s.n2, s.precision))
+                return FFT3D_B200_ERR_UNSUPPORTED;
+            persistent_ok = false;
+            continue;
         }
         BatchSeg d;
         d.in = s.in;
@@ -306,12 +314,20 @@ extern "C" int fft3d_b200_batch_create(const fft3d_b200_segment *segs, int nseg,
         if (prev >= 0) cudaSetDevice(prev);
         return code;
     };
-    if (cudaFuncSetAttribute(kc.func, cudaFuncAttributeMaxDynamicSharedMemorySize, kc.smem) != cudaSuccess)
+    if (!persistent_ok) {
+        items.clear();
+        dsegs.clear();
+        scratch_need = 0;
+        b->nitems = 0;
+    }
+    if (persistent_ok &&
+        cudaFuncSetAttribute(kc.func, cudaFuncAttributeMaxDynamicSharedMemorySize, kc.smem) != cudaSuccess)
         return fail(FFT3D_B200_ERR_CUDA);
     int occ = 0, sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kc.func, kc.threads, (size_t)kc.smem) != cudaSuccess ||
-        occ < 1)
+    if (persistent_ok &&
+        (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kc.func, kc.threads, (size_t)kc.smem) != cudaSuccess ||
+         occ < 1))
         return fail(FFT3D_B200_ERR_UNSUPPORTED);
     b->grid = std::max(1, std::min(occ * sms, std::max(1, b->nitems)));
     if (cudaMalloc(&b->d_items, std::max<size_t>(1, items.size()) * sizeof(BatchItem)) != cudaSuccess ||
@@ -337,7 +353,7 @@ extern "C" int fft3d_b200_batch_create(const fft3d_b200_segment *segs, int nseg,
     b->use_graph = !(flags & FFT3D_B200_FLAG_NO_GRAPH);
     if (cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking) != cudaSuccess)
         return fail(FFT3D_B200_ERR_CUDA);
-    if (b->use_graph) {
+    if (b->use_graph && persistent_ok) {
         if (cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
             return fail(FFT3D_B200_ERR_CUDA);
         cudaError_t le = batch_enqueue(b, b->cap);
@@ -347,7 +363,7 @@ extern "C" int fft3d_b200_batch_create(const fft3d_b200_segment *segs, int nseg,
     }
     // The per-segment strategy: built unless the persistent kernel is pinned
     // (or timing is off), then timed against the persistent launch.
-    const bool want_seg = (flags & FFT3D_B200_BATCH_SEGMENTS) ||
+    const bool want_seg = !persistent_ok || (flags & FFT3D_B200_BATCH_SEGMENTS) ||
                           !(flags & (FFT3D_B200_BATCH_PERSISTENT | FFT3D_B200_FLAG_NO_TUNE));
     float t_persist = -1.f, t_seg = -1.f;
     bool plans_ok = want_seg && nseg > 0;
@@ -367,7 +383,7 @@ extern "C" int fft3d_b200_batch_create(const fft3d_b200_segment *segs, int nseg,
             plans_ok = fft3d_b200_plan_create(&d, &b->plans[i]) == FFT3D_B200_OK;
         }
         if (!plans_ok) {  // a geometry without a plan: the persistent kernel only
-            if (flags & FFT3D_B200_BATCH_SEGMENTS) return fail(FFT3D_B200_ERR_UNSUPPORTED);
+            if ((flags & FFT3D_B200_BATCH_SEGMENTS) || !persistent_ok) return fail(FFT3D_B200_ERR_UNSUPPORTED);
             for (auto *pl : b->plans)
                 if (pl) fft3d_b200_plan_destroy(pl);
             b->plans.clear();
@@ -393,7 +409,7 @@ extern "C" int fft3d_b200_batch_create(const fft3d_b200_segment *segs, int nseg,
             if (cudaGraphInstantiate(&b->sexec, b->sgraph, 0) != cudaSuccess) return fail(FFT3D_B200_ERR_CUDA);
         }
         b->segments = true;
-        if (!(flags & FFT3D_B200_BATCH_SEGMENTS)) {
+        if (!(flags & FFT3D_B200_BATCH_SEGMENTS) && persistent_ok) {
             // the race, on the batch's own buffers
             t_seg = strategy_time_ms(b, true, b->cap, 5);
             t_persist = strategy_time_ms(b, false, b->cap, 5);

@@ -201,3 +201,28 @@ def test_timed_choice_is_reported_and_correct():
     for k, (shape, x, d, p) in enumerate(specs):
         err = oracle.rel_error_per_volume(outs[k].cpu().numpy().astype(np.complex128), ref(x, d))
         assert err.max() < (C128_TOL if p == fb.C128 else C64_TOL), (shape, err.max())
+
+
+def test_extents_without_a_persistent_kind_run_per_segment():
+    """Extents the persistent kernel has no kind for (the reference's other test
+    geometries) still batch: the batch runs one tuned plan per segment; pinning
+    the persistent kernel refuses them."""
+    rng = np.random.default_rng(61)
+    specs = []
+    for shape, n, d, p in [((9, 9, 9), 37, fb.FORWARD, fb.C128),
+                           ((7, 11, 13), 11, fb.BACKWARD, fb.C64),
+                           ((8, 8, 8), 100, fb.FORWARD, fb.C128),
+                           ((2, 3, 5), 300, fb.BACKWARD, fb.C128)]:
+        dt = np.complex128 if p == fb.C128 else np.complex64
+        specs.append((shape, field(rng, (n,) + shape, dtype=dt), d, p))
+    batch, ins, outs = make_batch(specs)
+    assert "per segment" in batch.describe()
+    batch.execute()
+    torch.cuda.synchronize()
+    for (shape, x, d, p), o in zip(specs, outs):
+        err = oracle.rel_error_per_volume(o.cpu().numpy(), ref(x, d)).max()
+        assert err < (C128_TOL if p == fb.C128 else C64_TOL), (shape, err)
+    batch.close()
+    with pytest.raises(fb.Fft3dError) as e:
+        make_batch(specs[:1], flags=fb.BATCH_PERSISTENT)
+    assert e.value.status == fb.ERR_UNSUPPORTED

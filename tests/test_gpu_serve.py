@@ -73,6 +73,10 @@ def test_stream_results_match_oracle_and_alone(flags):
     assert st["p99_s"] >= st["p50_s"] > 0
     if flags == 0:
         assert st["launches"] <= len(reqs)
+    # per-request latencies: one per finished request, every ticket once
+    lt, lat = srv.latencies()
+    assert sorted(int(t) for t in lt) == sorted(tickets)
+    assert (lat > 0).all() and float(np.percentile(lat, 50)) == pytest.approx(st["p50_s"], rel=0.5)
     srv.close()
     torch.cuda.synchronize()
     for r, x, xi, xo in work:
@@ -90,6 +94,30 @@ def test_stream_results_match_oracle_and_alone(flags):
             torch.cuda.synchronize()
             assert torch.equal(alone, xo), r
             b.close()
+
+
+def test_queued_requests_carry_their_wait():
+    """submit_many with arrival times (latency counts from when a request was
+    due): 32 requests due at once on one stream slot run one after another, so
+    the per-request latencies grow along the queue."""
+    rng = np.random.default_rng(9)
+    x = field(rng, (64, 17, 17, 17), "uniform", np.complex128)
+    xi = torch.from_numpy(x).cuda()
+    outs = [torch.empty_like(xi) for _ in range(32)]
+    srv = fb.Server(budget_bytes=64 << 30, max_inflight=1, flags=fb.SERVE_PLAIN)
+    segs = [{"shape": (17, 17, 17), "batch": 64, "in": xi.data_ptr(), "out": o.data_ptr()}
+            for o in outs]
+    # all 32 due at t = 0: one at a time on one slot, so the last waits for the others
+    srv.submit_many(segs, [0.0] * len(segs))
+    srv.drain(60)
+    tk, lat = srv.latencies()
+    order = np.argsort(tk)
+    lat = lat[order]
+    assert lat[-1] > lat[0]
+    assert lat[-1] >= 0.5 * lat.sum() / len(lat)
+    srv.close()
+    torch.cuda.synchronize()
+    assert oracle.rel_error_per_volume(outs[-1].cpu().numpy(), oracle.fft3d(x)).max() < C128_TOL
 
 
 def test_admission_budget_and_refusals():

@@ -258,7 +258,10 @@ int fft3d_b200_server_create(size_t hbm_budget_bytes, int max_inflight, unsigned
                              fft3d_b200_server **out);
 
 /* Queue one request (thread-safe).  FFT3D_B200_ERR_BUDGET if it alone exceeds
- * the budget.  `ticket` identifies it in fft3d_b200_server_poll. */
+ * the budget.  `ticket` identifies it in fft3d_b200_server_poll.  Extents of the
+ * persistent batch kernel are coalesced; any other extent with a kernel that
+ * needs no plan workspace is served by its own launch in the same slot, and
+ * the rest (45^3, 64^3) are refused with FFT3D_B200_ERR_UNSUPPORTED. */
 int fft3d_b200_server_submit(fft3d_b200_server *server, const fft3d_b200_segment *request,
                              unsigned long long *ticket);
 

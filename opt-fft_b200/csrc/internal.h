@@ -87,6 +87,9 @@ int entry_occupancy(const KernelEntry &e, int device);
 
 int element_bytes(int precision);
 
+// Whether a geometry has a kernel that needs no plan workspace (what tuned_entry
+// chooses among).
+bool has_workspace_free_kernel(int n0, int n1, int n2, int precision, int sign);
 // The autotuner's choice for a geometry at a batch size (memoised per batch
 // bucket like plan creation); nullptr if the geometry has no kernel.
 const KernelEntry *tuned_entry(int device, int n0, int n1, int n2, int precision, int sign,

@@ -322,6 +322,13 @@ static const KernelEntry *tune(const std::vector<const KernelEntry *> &cands, in
     return best ? best : cands[0];
 }
 
+bool has_workspace_free_kernel(int n0, int n1, int n2, int precision, int sign)
+{
+    for (const KernelEntry *k : candidates(n0, n1, n2, precision, sign))
+        if (k->family != FAM_TWOPASS) return true;
+    return false;
+}
+
 const KernelEntry *tuned_entry(int device, int n0, int n1, int n2, int precision, int sign,
                                long long batch)
 {

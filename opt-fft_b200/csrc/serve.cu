@@ -15,6 +15,10 @@
 // per-CTA scratch of the two-phase 36^3 route, allocated once at creation; the
 // hot loop allocates nothing on the device.
 //
+// A request whose extent is not one of the persistent kernel's kinds (any
+// other compiled extent with a kernel that needs no plan workspace) is
+// launched on its own with its tuned kernel, on the same stream as the batch.
+//
 // Baseline mode (FFT3D_B200_SERVE_PLAIN): every request is launched on its own,
 // as soon as it is admitted, with the tuned per-geometry kernel of its kind --
 // one launch per request.
@@ -131,6 +135,18 @@ static int launch_slot(fft3d_b200_server *s, ServeSlot &slot)
                 return FFT3D_B200_ERR_CUDA;
         }
     } else {
+        // requests whose extent is not a kind of the persistent kernel: one
+        // tuned launch each on the slot's stream, beside the batch launch
+        for (const ServeReq &r : slot.reqs) {
+            if (r.kind >= 0) continue;
+            int grid = 0;
+            const KernelEntry *e = plain_entry(s, r, &grid);
+            if (!e) return FFT3D_B200_ERR_UNSUPPORTED;
+            const double scale = r.seg.direction == FFT3D_B200_BACKWARD ? 1.0 / (double)r.vol_elems : 1.0;
+            if (launch_entry(*e, r.seg.in, r.seg.out, r.seg.batch, scale, st, grid, slot.d_err) !=
+                cudaSuccess)
+                return FFT3D_B200_ERR_CUDA;
+        }
         // descriptors: requests are segments; items largest first
         int nseg = (int)slot.reqs.size();
         std::vector<int> order(nseg);
@@ -151,8 +167,12 @@ static int launch_slot(fft3d_b200_server *s, ServeSlot &slot)
             d.out = r.seg.out;
             d.scale = r.seg.direction == FFT3D_B200_BACKWARD ? 1.0 / (double)r.vol_elems : 1.0;
             d.nvol = r.seg.batch;
-            d.kind = r.kind;
+            d.kind = r.kind < 0 ? 0 : r.kind;
             d.pad = 0;
+            if (r.kind < 0) {
+                d.nvol = 0;  // launched on its own above; no item refers to it
+                continue;
+            }
             int so = 0;
             batch_kind_of(r.seg.n0, r.seg.n1, r.seg.n2, r.seg.precision, r.seg.direction, nullptr,
                           nullptr, nullptr, &so);
@@ -161,6 +181,7 @@ static int launch_slot(fft3d_b200_server *s, ServeSlot &slot)
         for (int oi = 0; oi < nseg; ++oi) {
             const int i = order[oi];
             const ServeReq &r = slot.reqs[i];
+            if (r.kind < 0) continue;
             for (long long v0 = 0; v0 < r.seg.batch; v0 += r.vpc) {
                 BatchItem &it = slot.h_items[n++];
                 it.kind = r.kind;
@@ -170,13 +191,13 @@ static int launch_slot(fft3d_b200_server *s, ServeSlot &slot)
                 it.pad = 0;
             }
         }
-        if (n == 0) return FFT3D_B200_OK;
-        if (cudaMemcpyAsync(slot.d_items, slot.h_items, (size_t)n * sizeof(BatchItem),
-                            cudaMemcpyHostToDevice, st) != cudaSuccess ||
-            cudaMemcpyAsync(slot.d_segs, slot.h_segs, (size_t)nseg * sizeof(BatchSeg),
-                            cudaMemcpyHostToDevice, st) != cudaSuccess ||
-            cudaMemcpyAsync(slot.d_solo, solo, sizeof solo, cudaMemcpyHostToDevice, st) != cudaSuccess ||
-            cudaMemsetAsync(slot.d_ticket, 0, sizeof(unsigned int), st) != cudaSuccess)
+        if (n > 0 &&
+            (cudaMemcpyAsync(slot.d_items, slot.h_items, (size_t)n * sizeof(BatchItem),
+                             cudaMemcpyHostToDevice, st) != cudaSuccess ||
+             cudaMemcpyAsync(slot.d_segs, slot.h_segs, (size_t)nseg * sizeof(BatchSeg),
+                             cudaMemcpyHostToDevice, st) != cudaSuccess ||
+             cudaMemcpyAsync(slot.d_solo, solo, sizeof solo, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+             cudaMemsetAsync(slot.d_ticket, 0, sizeof(unsigned int), st) != cudaSuccess))
             return FFT3D_B200_ERR_CUDA;
         const BatchItem *items = slot.d_items;
         const BatchSeg *segs = slot.d_segs;
@@ -188,8 +209,8 @@ static int launch_slot(fft3d_b200_server *s, ServeSlot &slot)
         int grid = std::min(s->grid, n);
         void *args[] = {(void *)&items, (void *)&n,       (void *)&segs, (void *)&ticket,
                         (void *)&scratch, (void *)&spc, (void *)&so,   (void *)&err};
-        if (cudaLaunchKernel(batch_kernel_func(), dim3(grid), dim3(batch_kernel_threads()), args,
-                             (size_t)batch_kernel_smem(), st) != cudaSuccess)
+        if (n > 0 && cudaLaunchKernel(batch_kernel_func(), dim3(grid), dim3(batch_kernel_threads()), args,
+                                      (size_t)batch_kernel_smem(), st) != cudaSuccess)
             return FFT3D_B200_ERR_CUDA;
     }
     if (cudaEventRecord(slot.done, st) != cudaSuccess) return FFT3D_B200_ERR_CUDA;
@@ -366,14 +387,21 @@ static int server_submit_at(fft3d_b200_server *s, const fft3d_b200_segment *req,
     r.seg = q;
     r.kind = batch_kind_of(q.n0, q.n1, q.n2, q.precision, q.direction, &r.vpc, &r.big,
                            &r.vol_elems, nullptr);
-    if (r.kind < 0) return FFT3D_B200_ERR_UNSUPPORTED;
+    if (r.kind < 0) {
+        // not a kind of the persistent kernel: served by its own tuned launch
+        if (!has_workspace_free_kernel(q.n0, q.n1, q.n2, q.precision, q.direction))
+            return FFT3D_B200_ERR_UNSUPPORTED;
+        r.vpc = 1;
+        r.big = 0;
+        r.vol_elems = (long long)q.n0 * q.n1 * q.n2;
+    }
     const size_t eb = (size_t)element_bytes(q.precision);
     r.bytes = 2 * (size_t)q.batch * (size_t)r.vol_elems * eb;
     if (((uintptr_t)q.in % eb) || ((uintptr_t)q.out % eb)) return FFT3D_B200_ERR_ALIGN;
     const char *a = (const char *)q.in, *o = (const char *)q.out;
     if (a < o + r.bytes / 2 && o < a + r.bytes / 2) return FFT3D_B200_ERR_OVERLAP;
     if (r.bytes > s->budget) return FFT3D_B200_ERR_BUDGET;
-    r.nitems = (q.batch + r.vpc - 1) / r.vpc;
+    r.nitems = r.kind < 0 ? 0 : (q.batch + r.vpc - 1) / r.vpc;
     if (r.nitems > SERVE_MAX_ITEMS) return FFT3D_B200_ERR_BUDGET;
     {
         std::lock_guard<std::mutex> lk(s->mu);

@@ -148,3 +148,39 @@ def test_admission_budget_and_refusals():
         srv.submit({"shape": (7, 7, 7), "batch": 1, "in": big.data_ptr(), "out": bo.data_ptr()})
     assert e.value.status == fb.ERR_UNSUPPORTED
     srv.close()
+
+
+def test_extents_outside_the_batch_kinds():
+    """Extents that are not kinds of the persistent batch kernel (9^3, 7x11x13,
+    2x3x5, 32x8x4 here) are served by their own tuned launch in the same slot
+    as the coalesced kinds; every result matches the oracle, and an extent whose
+    only kernels need a plan workspace (45^3) is refused."""
+    rng = np.random.default_rng(11)
+    specs = [((9, 9, 9), fb.C128, fb.FORWARD, 5), ((7, 11, 13), fb.C64, fb.BACKWARD, 3),
+             ((17, 17, 17), fb.C128, fb.FORWARD, 4), ((2, 3, 5), fb.C128, fb.BACKWARD, 7),
+             ((8, 8, 8), fb.C64, fb.FORWARD, 30), ((32, 8, 4), fb.C64, fb.FORWARD, 2),
+             ((9, 9, 9), fb.C64, fb.BACKWARD, 2), ((12, 12, 12), fb.C128, fb.BACKWARD, 6)]
+    work = []
+    for shape, prec, d, b in specs:
+        dt = np.complex128 if prec == fb.C128 else np.complex64
+        x = field(rng, (b,) + shape, "uniform", dt)
+        xi = torch.from_numpy(x).cuda()
+        work.append((shape, prec, d, x, xi, torch.full_like(xi, complex(3.0, 3.0))))
+    srv = fb.Server(budget_bytes=8 << 30, max_inflight=2)
+    tickets = [srv.submit({"shape": s, "batch": x.shape[0], "direction": d, "precision": p,
+                           "in": xi.data_ptr(), "out": xo.data_ptr()})
+               for s, p, d, x, xi, xo in work]
+    srv.drain(60)
+    assert srv.stats()["requests"] == len(work)
+    lt, lat = srv.latencies()
+    assert sorted(int(t) for t in lt) == sorted(tickets)
+    big = torch.zeros(2 * 45 ** 3, dtype=torch.complex128, device="cuda")
+    bo = torch.zeros_like(big)
+    with pytest.raises(fb.Fft3dError) as e:
+        srv.submit({"shape": (45, 45, 45), "batch": 2, "in": big.data_ptr(), "out": bo.data_ptr()})
+    assert e.value.status == fb.ERR_UNSUPPORTED
+    srv.close()
+    torch.cuda.synchronize()
+    for s, p, d, x, xi, xo in work:
+        err = oracle.rel_error_per_volume(xo.cpu().numpy().astype(np.complex128), ref(x, d))
+        assert err.max() < (C128_TOL if p == fb.C128 else C64_TOL), (s, p, d, err.max())

@@ -69,8 +69,8 @@ struct BatchSeg {
 constexpr int BATCH_NKINDS = 36;
 
 // The complex64 kinds for the class-1 kernel (two CTAs per SM, half the shared
-// memory each): the same ids, volumes per item re-sized for a 57 KB half, and
-// 24^3 (115 KB a volume) through the two-phase route as well.
+// memory each): the same ids, volumes per item re-sized for a 57 KB half; a
+// 24^3 volume (115,200 bytes with its row padding) takes a CTA's whole share.
 #define FFT3D_BATCH_KINDS_C64(X)                     \
     X(18, 6, 6, 6, float, -1, 28, 0, 0)              \
     X(19, 6, 6, 6, float, +1, 28, 0, 0)              \
@@ -82,8 +82,8 @@ constexpr int BATCH_NKINDS = 36;
     X(25, 16, 16, 16, float, +1, 1, 0, 0)            \
     X(26, 17, 17, 17, float, -1, 1, 0, 0)            \
     X(27, 17, 17, 17, float, +1, 1, 0, 0)            \
-    X(28, 24, 24, 24, float, -1, 1, 1, 12)           \
-    X(29, 24, 24, 24, float, +1, 1, 1, 12)           \
+    X(28, 24, 24, 24, float, -1, 1, 1, 0)            \
+    X(29, 24, 24, 24, float, +1, 1, 1, 0)            \
     X(30, 36, 36, 36, float, -1, 1, 1, 9)            \
     X(31, 36, 36, 36, float, +1, 1, 1, 9)            \
     X(32, 8, 8, 16, float, -1, 7, 0, 0)              \

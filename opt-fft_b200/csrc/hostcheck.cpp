@@ -119,6 +119,26 @@ static void emulate_big_cube(const void *vin, void *vout, long long nvol)
 
 static long long g_twopass_violations = 0;
 
+// The ring as the kernels see it: 128-byte aligned, filled with a marker.
+template <typename T>
+static cx<T> *aligned_ring(std::vector<cx<T>> &buf, long long elems)
+{
+    buf.assign((size_t)elems + 128 / sizeof(cx<T>), cx<T>{T(-777.0), T(555.0)});
+    return reinterpret_cast<cx<T> *>(((uintptr_t)buf.data() + 127) & ~(uintptr_t)127);
+}
+
+// A row item's discards (twopass_kernels.cu twopass_discard_rows): the lines
+// it drops hold garbage afterwards, so a later read of one shows up as NaN.
+template <class TG>
+static void poison_discarded_rows(void *slot, int j)
+{
+    constexpr int NQ = TG::YG::N0 * twopass_row_lines_per_plane<TG>();
+    for (int q = 0; q < NQ; ++q) {
+        uintptr_t line;
+        if (twopass_row_line<TG>(slot, j, q, &line)) memset((void *)line, 0xff, 128);
+    }
+}
+
 // The TWOPASS kernel's work items (twopass_kernels.cu k_twopass), taken in
 // ticket order with the kernel's decode, element maps and ring of R slots.
 // Ticket order satisfies every dependency, so one "CTA" can run them in turn;
@@ -132,7 +152,8 @@ static void emulate_twopass(const void *vin, void *vout, long long nvol)
     const T scale = S > 0 ? T(1) / T(TG::V) : T(1);
     int lag = 0;
     const int R = twopass_ring_size(TG::NA, TG::NB, 7, &lag);
-    std::vector<cx<T>> sm((size_t)TG::PV), ring((size_t)R * TG::V, cx<T>{T(-777.0), T(555.0)});
+    std::vector<cx<T>> sm((size_t)TG::PV), ringbuf;
+    cx<T> *ring = aligned_ring(ringbuf, (long long)R * TG::V);
     const cx<T> *in = (const cx<T> *)vin;
     cx<T> *out = (cx<T> *)vout;
     const long long total = (long long)(TG::NA + TG::NB) * nvol;
@@ -141,7 +162,7 @@ static void emulate_twopass(const void *vin, void *vout, long long nvol)
         const TwoPassItem it = twopass_decode(t, nvol, TG::NA, TG::NB, lag);
         const int slot = (int)(it.vol % R);
         const long long round = it.vol / R;
-        cx<T> *sv = ring.data() + slot * TG::V;
+        cx<T> *sv = ring + slot * TG::V;
         for (auto &e : sm) e = {T(12345.0), T(-6789.0)};
         // the kernel's waits must already hold in ticket order
         if (it.plane ? cnt_row[slot] < TG::NB * round : cnt_plane[slot] < TG::NA * (round + 1))
@@ -169,6 +190,7 @@ static void emulate_twopass(const void *vin, void *vout, long long nvol)
                 twopass_row_elem<TG>(it.j, g, &vo, &so);
                 sm[so] = sv[vo];
             }
+            poison_discarded_rows<TG>(sv, it.j);
             for (int l = 0; l < G * N2; ++l)
                 pass_x_slab<YG, S, N1>(sm.data(), l, out + it.vol * TG::V, it.j * G, scale);
         }
@@ -188,7 +210,8 @@ static void emulate_twopass_regs(const void *vin, void *vout, long long nvol)
     const T scale = S > 0 ? T(1) / T(TG::V) : T(1);
     int lag = 0;
     const int R = twopass_ring_size(TG::NA, TG::NB, 7, &lag);
-    std::vector<cx<T>> sm((size_t)TG::PV), ring((size_t)R * TG::V, cx<T>{T(-777.0), T(555.0)});
+    std::vector<cx<T>> sm((size_t)TG::PV), ringbuf;
+    cx<T> *ring = aligned_ring(ringbuf, (long long)R * TG::V);
     const cx<T> *in = (const cx<T> *)vin;
     cx<T> *out = (cx<T> *)vout;
     const long long total = (long long)(TG::NA + TG::NB) * nvol;
@@ -197,7 +220,7 @@ static void emulate_twopass_regs(const void *vin, void *vout, long long nvol)
         const TwoPassItem it = twopass_decode(t, nvol, TG::NA, TG::NB, lag);
         const int slot = (int)(it.vol % R);
         const long long round = it.vol / R;
-        cx<T> *sv = ring.data() + slot * TG::V;
+        cx<T> *sv = ring + slot * TG::V;
         if (it.plane ? cnt_row[slot] < TG::NB * round : cnt_plane[slot] < TG::NA * (round + 1))
             g_twopass_violations++;
         (it.plane ? cnt_plane : cnt_row)[slot]++;
@@ -214,11 +237,13 @@ static void emulate_twopass_regs(const void *vin, void *vout, long long nvol)
                 for (int z = 0; z < N2; ++z)
                     sm[YG::off(q, z)] = sv[((long long)x * N1 + it.j * G + yl) * N2 + z];
             }
+            poison_discarded_rows<TG>(sv, it.j);
             for (int l = 0; l < G * N2; ++l)
                 pass_x_slab<YG, S, N1>(sm.data(), l, out + it.vol * TG::V, it.j * G, scale);
         } else {
             for (int l = 0; l < G * N2; ++l)
                 pass_x_load_l2<N0, N1, N2, S, T>(sv, l, out + it.vol * TG::V, it.j * G, scale);
+            poison_discarded_rows<TG>(sv, it.j);
         }
     }
 }
@@ -239,7 +264,8 @@ static void emulate_twopass_lanes(const void *vin, void *vout, long long nvol)
     const T scale = S > 0 ? T(1) / T(TG::V) : T(1);
     int lag = 0;
     const int R = twopass_ring_size(TG::NA, TG::NB, 7, &lag);
-    std::vector<cx<T>> sm((size_t)TG::PV), ring((size_t)R * TG::V, cx<T>{T(-777.0), T(555.0)});
+    std::vector<cx<T>> sm((size_t)TG::PV), ringbuf;
+    cx<T> *ring = aligned_ring(ringbuf, (long long)R * TG::V);
     const cx<T> *in = (const cx<T> *)vin;
     cx<T> *out = (cx<T> *)vout;
     const long long total = (long long)(TG::NA + TG::NB) * nvol;
@@ -248,7 +274,7 @@ static void emulate_twopass_lanes(const void *vin, void *vout, long long nvol)
         const TwoPassItem it = twopass_decode(tk, nvol, TG::NA, TG::NB, lag);
         const int slot = (int)(it.vol % R);
         const long long round = it.vol / R;
-        cx<T> *sv = ring.data() + slot * TG::V;
+        cx<T> *sv = ring + slot * TG::V;
         if (it.plane ? cnt_row[slot] < TG::NB * round : cnt_plane[slot] < TG::NA * (round + 1))
             g_twopass_violations++;
         (it.plane ? cnt_plane : cnt_row)[slot]++;
@@ -274,6 +300,7 @@ static void emulate_twopass_lanes(const void *vin, void *vout, long long nvol)
                 const int x = q / G, yl = q % G;
                 for (int z = 0; z < N; ++z) sm[YG::off(q, z)] = sv[((long long)x * N + it.j * G + yl) * N + z];
             }
+            poison_discarded_rows<TG>(sv, it.j);
             cx<T> *gvol = out + it.vol * TG::V;
             for (int l = 0; l < LINES; ++l) {
                 const int yl = l / N, z = l % N;
@@ -303,7 +330,8 @@ static void emulate_twopass_staged(const void *vin, void *vout, long long nvol)
     const T scale = S > 0 ? T(1) / T(TG::V) : T(1);
     int lag = 0;
     const int R = twopass_ring_size(TG::NA, TG::NB, 7, &lag);
-    std::vector<cx<T>> smv((size_t)N * P), ring((size_t)R * TG::V, cx<T>{T(-777.0), T(555.0)});
+    std::vector<cx<T>> smv((size_t)N * P), ringbuf;
+    cx<T> *ring = aligned_ring(ringbuf, (long long)R * TG::V);
     cx<T> *sm = smv.data();
     const cx<T> *in = (const cx<T> *)vin;
     cx<T> *out = (cx<T> *)vout;
@@ -315,7 +343,7 @@ static void emulate_twopass_staged(const void *vin, void *vout, long long nvol)
         const TwoPassItem it = twopass_decode(t, nvol, TG::NA, TG::NB, lag);
         const int slot = (int)(it.vol % R);
         const long long round = it.vol / R;
-        cx<T> *sv = ring.data() + slot * TG::V;
+        cx<T> *sv = ring + slot * TG::V;
         if (it.plane ? cnt_row[slot] < TG::NB * round : cnt_plane[slot] < TG::NA * (round + 1))
             g_twopass_violations++;
         (it.plane ? cnt_plane : cnt_row)[slot]++;
@@ -334,6 +362,7 @@ static void emulate_twopass_staged(const void *vin, void *vout, long long nvol)
         } else {
             for (int x = 0; x < N; ++x)
                 for (int z = 0; z < N; ++z) sm[x * P + z] = sv[((long long)x * N + it.j) * N + z];
+            poison_discarded_rows<TG>(sv, it.j);
             for (int q = 0; q < N * Line::T1; ++q) Line::template stage1<S, T>(sm, N, q, coladdr);
             cx<T> *gvol = out + it.vol * TG::V + (long long)it.j * N;
             for (int q = 0; q < N * Line::T2; ++q)

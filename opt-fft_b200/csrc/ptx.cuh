@@ -178,6 +178,14 @@ __device__ __forceinline__ void st_cg_hint(float2 *p, float2 v, uint64_t policy)
                  : "memory");
 }
 
+// Drop the 128-byte L2 line at p (128-byte aligned) without writing it back;
+// its contents become undefined.  For scratch read for the last time, so that
+// its dirty lines never reach HBM.
+__device__ __forceinline__ void discard_l2_line(uintptr_t p)
+{
+    asm volatile("discard.global.L2 [%0], 128;" ::"l"(p) : "memory");
+}
+
 // Per-thread asynchronous copies global -> shared (cp.async, 16 or 8 bytes).
 __device__ __forceinline__ void cp_async_16(void *dst, const void *src)
 {

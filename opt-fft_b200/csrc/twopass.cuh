@@ -37,6 +37,30 @@ struct TwoPassGeom {
     static constexpr int ROW_ELEMS = N0 * G * N2;    // elements of a row item
 };
 
+// The 128-byte lines of scratch that a row item (v, j) may drop from L2 once
+// it has read its rows for the last time: in each x-plane x, the whole lines
+// inside its G consecutive y-rows [j*G, (j+1)*G) (a line shared with a
+// neighbouring item's rows is kept -- that item may not have read it yet).
+// Line index q runs over [0, N0 * twopass_row_lines_per_plane<TG>()); false
+// when q names no whole line.
+template <class TG>
+FFT_HD constexpr int twopass_row_lines_per_plane()
+{
+    return TG::YG::N1 * TG::YG::N2 * TG::XG::EB / 128 + 1;
+}
+
+template <class TG>
+FFT_HD bool twopass_row_line(const void *slot, int j, int q, uintptr_t *line)
+{
+    constexpr int G = TG::YG::N1, N2 = TG::YG::N2, PER = twopass_row_lines_per_plane<TG>();
+    constexpr long long EB = TG::XG::EB;
+    const int x = q / PER, k = q % PER;
+    const uintptr_t a = (uintptr_t)slot + (uintptr_t)(((long long)x * TG::N1F + (long long)j * G) * N2 * EB);
+    const uintptr_t first = (a + 127) & ~(uintptr_t)127;
+    *line = first + (uintptr_t)k * 128;
+    return *line + 128 <= a + (uintptr_t)(G * N2 * EB);
+}
+
 struct TwoPassItem {
     bool plane;
     long long vol;

@@ -30,6 +30,19 @@
 
 namespace fft3d {
 
+// Every thread: drop from L2, without a write-back, the scratch lines whose
+// rows row item j has read for the last time (twopass_row_line).  A barrier
+// must follow before the slot is released to the next volume's plane items.
+template <class TG>
+__device__ __forceinline__ void twopass_discard_rows(const void *slot, int j, int tid, int nt)
+{
+    constexpr int NQ = TG::YG::N0 * twopass_row_lines_per_plane<TG>();
+    for (int q = tid; q < NQ; q += nt) {
+        uintptr_t line;
+        if (twopass_row_line<TG>(slot, j, q, &line)) discard_l2_line(line);
+    }
+}
+
 template <typename T>
 __device__ __forceinline__ cx<T> ld_l2(const cx<T> *p)
 {
@@ -142,7 +155,10 @@ __global__ void __launch_bounds__(NT, MINB)
                     if (so[u] >= 0) sm[so[u]] = v[u];
             }
             __syncthreads();
-            // the slot may be overwritten once every row item has read it
+            // read for the last time: drop the rows from L2 unwritten; then the
+            // slot may be overwritten once every row item has read it
+            twopass_discard_rows<TG>(sv, it.j, tid, NT);
+            __syncthreads();
             if (tid == 0) red_release_gpu_add(&ctl->cnt[TWOPASS_RMAX + slot], 1u);
             // 3. x pass, straight to the output
             cx<T> *gvol = out + it.vol * TG::V;
@@ -276,7 +292,10 @@ __global__ void __launch_bounds__(NT, MINB)
             __syncthreads();  // then one cumulative release publishes every thread's stores
             if (tid == 0) red_release_gpu_add(&ctl->cnt[slot], 1u);
         } else {
-            // the copies of this row item are complete: its slot may be reused
+            // the copies of this row item are complete: drop its rows from L2
+            // unwritten, then the slot may be reused
+            twopass_discard_rows<TG>(sv, it.j, tid, NT);
+            __syncthreads();
             if (tid == 0) red_release_gpu_add(&ctl->cnt[TWOPASS_RMAX + slot], 1u);
             cx<T> *gvol = out + it.vol * TG::V;
             for (int l = tid; l < G * N2; l += NT) pass_x_slab<YG, S, N1>(sm, l, gvol, it.j * G, scale);
@@ -454,7 +473,10 @@ __global__ void __launch_bounds__(NT, MINB)
             if (!wait_copies()) s_stop = 2;
             __syncthreads();
             if (s_stop) break;
-            // the slot may be overwritten: its rows are in shared memory
+            // its rows are in shared memory: drop them from L2 unwritten, then
+            // the slot may be overwritten
+            twopass_discard_rows<TG>(sv, it.j, tid, NT);
+            __syncthreads();
             if (tid == 0) red_release_gpu_add(&ctl->cnt[TWOPASS_RMAX + slot], 1u);
             // 2. x pass, straight to the output
             for (int l = tid; l < G * N2; l += NT)
@@ -466,6 +488,8 @@ __global__ void __launch_bounds__(NT, MINB)
             for (int l = tid; l < G * N2; l += NT)
                 pass_x_load_l2<N0, N1, N2, S, T>(sv, l, out + it.vol * TG::V, it.j * G, scale);
             __syncthreads();  // every load of the slot has returned
+            twopass_discard_rows<TG>(sv, it.j, tid, NT);
+            __syncthreads();
             if (tid == 0) red_release_gpu_add(&ctl->cnt[TWOPASS_RMAX + slot], 1u);
         }
     }
@@ -617,6 +641,10 @@ __global__ void __launch_bounds__(NT, MINB)
             if (!wait_copies()) s_stop = 2;
             __syncthreads();
             if (s_stop) break;
+            // its rows are in shared memory: drop them from L2 unwritten, then
+            // the slot may be overwritten
+            twopass_discard_rows<TG>(sv, it.j, tid, NT);
+            __syncthreads();
             if (tid == 0) red_release_gpu_add(&ctl->cnt[TWOPASS_RMAX + slot], 1u);
             // 2. x pass, straight to the output: line = (yl, z)
             cx<T> *gvol = out + it.vol * TG::V;
@@ -780,7 +808,10 @@ __global__ void __launch_bounds__(NT, MINB)
             if (!wait_copies()) s_stop = 2;
             __syncthreads();
             if (s_stop) break;
-            // the slot may be overwritten: its rows are in shared memory
+            // its rows are in shared memory: drop them from L2 unwritten, then
+            // the slot may be overwritten
+            twopass_discard_rows<TG>(sv, it.j, tid, NT);
+            __syncthreads();
             if (tid == 0) red_release_gpu_add(&ctl->cnt[TWOPASS_RMAX + slot], 1u);
             // 2. x pass along the columns (column z), streamed to the output
             for (int t = tid; t < N * Line::T1; t += NT) Line::template stage1<S, T>(sm, N, t, coladdr);

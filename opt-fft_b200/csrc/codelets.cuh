@@ -101,11 +101,15 @@ constexpr int tw_off(int n) { return n * (n - 1) / 2; }   // N = 1..TW_MAXN, pac
 constexpr int TW_ENTRIES = tw_off(TW_MAXN + 1);            // 2080
 // Rader-17 kernel spectra: [sign index][16], sign index 0 = forward, 1 = backward.
 constexpr int RADER17_ENTRIES = 32;
-// Line lengths above TW_MAXN (lines spread over several lanes): one table per N
-// in global memory, read through the read-only cache (lane-dependent indices
-// would serialise on the constant cache).
-constexpr int twbig_off(int n) { return n == 96 ? 0 : n == 128 ? 96 : n == 192 ? 224 : n == 256 ? 416 : -1; }
-constexpr int TWBIG_ENTRIES = 672;
+// Line lengths above TW_MAXN: one table per N in global memory, read through
+// the read-only cache -- lines spread over several lanes (96..256; lane-dependent
+// indices would serialise on the constant cache) and the primes 83 and 97 of the
+// reference's test geometries (folded direct sums).
+constexpr int twbig_off(int n)
+{
+    return n == 96 ? 0 : n == 128 ? 96 : n == 192 ? 224 : n == 256 ? 416 : n == 83 ? 672 : n == 97 ? 755 : -1;
+}
+constexpr int TWBIG_ENTRIES = 852;
 
 }  // namespace fft3d
 
@@ -206,6 +210,15 @@ FFT_HD cx<T> cmul_iS(cx<T> a)
     else return {a.im, -a.re};
 }
 
+// {cos, sin}(2*pi*e/N), 0 <= e < N, from the table that holds N.
+template <int N, typename T>
+FFT_HD auto line_tw(int e)
+{
+    static_assert(N <= TW_MAXN || twbig_off(N) >= 0, "no twiddle table for this extent");
+    if constexpr (N <= TW_MAXN) return Tab<T>::tw(tw_off(N) + e);
+    else return Tab<T>::twbig(twbig_off(N) + e);
+}
+
 // a * W_N^e with W_N = exp(S*2*pi*i/N).  Callers pass an exponent that is a
 // constant once their loops are unrolled, so the branches below fold away and
 // the table read becomes a constant-bank operand.
@@ -217,9 +230,7 @@ FFT_HD cx<T> ctwiddle(cx<T> a, int E)
     if (4 * e == N) return cmul_iS<S>(a);
     if (2 * e == N) return {-a.re, -a.im};
     if (4 * e == 3 * N) return cmul_iS<-S>(a);
-    static_assert(N <= TW_MAXN || twbig_off(N) >= 0, "no twiddle table for this extent");
-    const auto w = N <= TW_MAXN ? Tab<T>::tw(tw_off(N) + e)        // {cos, sin}(2*pi*e/N)
-                                : Tab<T>::twbig(twbig_off(N) + e);
+    const auto w = line_tw<N, T>(e);  // {cos, sin}(2*pi*e/N)
     const T c = w.x;
     const T s = (S > 0) ? w.y : -w.y;
     return {a.re * c - a.im * s, a.re * s + a.im * c};
@@ -256,7 +267,7 @@ FFT_HD void dft_odd_folded(cx<T> *v)
 #pragma unroll
         for (int j = 1; j <= H; ++j) {
             const int e = (j * k) % N;
-            const auto t = Tab<T>::tw(tw_off(N) + e);
+            const auto t = line_tw<N, T>(e);
             a.re += u[j].re * t.x;
             a.im += u[j].im * t.x;
             b.re += w[j].re * t.y;

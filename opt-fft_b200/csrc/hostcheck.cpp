@@ -450,6 +450,24 @@ static const EmuEntry kEmu[] = {
     EMU(2, 3, 5, float, 0, 64),   EMU(7, 11, 13, float, 0, 4),   EMU(5, 8, 12, float, 0, 8),
     EMU(13, 5, 8, float, 0, 8),   EMU(17, 2, 2, float, 0, 32),   EMU(32, 8, 4, float, 0, 4),
     EMU(1, 8, 8, float, 0, 64),   EMU(8, 1, 8, float, 0, 64),    EMU(8, 8, 1, float, 0, 64),
+    // the rest of the reference's test geometries, at their VOLUME group sizes
+    EMU(2, 2, 2, double, 0, 64),   EMU(5, 5, 5, double, 0, 24),  EMU(7, 7, 7, double, 0, 8),
+    EMU(11, 11, 11, double, 0, 2), EMU(49, 2, 2, double, 0, 10), EMU(25, 4, 3, double, 0, 10),
+    EMU(27, 2, 2, double, 0, 18),  EMU(19, 3, 2, double, 0, 17), EMU(23, 2, 2, double, 0, 22),
+    EMU(47, 3, 2, double, 0, 7),   EMU(83, 2, 1, double, 0, 18), EMU(97, 2, 1, double, 0, 15),
+    EMU(1, 1, 16, double, 0, 64),  EMU(1, 7, 1, double, 0, 64),  EMU(3, 5, 7, double, 0, 29),
+    EMU(4, 6, 10, double, 0, 11),  EMU(16, 3, 5, double, 0, 12), EMU(24, 18, 12, double, 0, 1),
+    EMU(2, 2, 64, double, 0, 12),  EMU(64, 2, 2, double, 0, 8),  EMU(9, 25, 7, double, 0, 1),
+    EMU(20, 12, 6, double, 0, 1),  EMU(11, 4, 9, double, 0, 7),
+    EMU(2, 2, 2, float, 0, 64),    EMU(5, 5, 5, float, 0, 49),   EMU(7, 7, 7, float, 0, 17),
+    EMU(11, 11, 11, float, 0, 4),  EMU(49, 2, 2, float, 0, 20),  EMU(25, 4, 3, float, 0, 20),
+    EMU(27, 2, 2, float, 0, 37),   EMU(19, 3, 2, float, 0, 35),  EMU(23, 2, 2, float, 0, 44),
+    EMU(47, 3, 2, float, 0, 14),   EMU(83, 2, 1, float, 0, 37),  EMU(97, 2, 1, float, 0, 31),
+    EMU(1, 1, 16, float, 0, 64),   EMU(1, 7, 1, float, 0, 64),   EMU(3, 5, 7, float, 0, 58),
+    EMU(4, 6, 10, float, 0, 23),   EMU(16, 3, 5, float, 0, 25),  EMU(24, 18, 12, float, 0, 1),
+    EMU(30, 30, 30, float, 0, 1),  EMU(2, 2, 64, float, 0, 24),  EMU(64, 2, 2, float, 0, 16),
+    EMU(9, 25, 7, float, 0, 3),    EMU(20, 12, 6, float, 0, 3),  EMU(11, 4, 9, float, 0, 15),
+    EMU_TP(30, 30, 30, double, 3), EMU_TP(30, 30, 30, double, 5),
 };
 
 // The chain kernel's per-CTA loop (chain_kernels.cu k_chain) for one volume per CTA.

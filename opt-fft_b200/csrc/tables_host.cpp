@@ -49,7 +49,7 @@ static void fill_host_tables()
             h_tw_f[tw_off(n) + e] = make_float2((float)c, (float)s);
         }
     }
-    for (int n : {96, 128, 192, 256}) {
+    for (int n : {96, 128, 192, 256, 83, 97}) {
         for (int e = 0; e < n; ++e) {
             long double c, s;
             exact_cis(e, n, &c, &s);

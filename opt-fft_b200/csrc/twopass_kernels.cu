@@ -1041,6 +1041,9 @@ void register_twopass_kernels(std::vector<KernelEntry> &out)
     FFT3D_TWOPASS_BULKQH(45, 45, 45, 5, 256, 1);
     FFT3D_TWOPASS_STAGED(LinePFA45, 45, double, "pfa", 128, 6);
     // 45^3 complex float (a 360-byte row cannot be a bulk copy): element copies
+    // 30^3 complex128 (446 KB a volume), a test geometry of the reference
+    FFT3D_TWOPASS(30, 30, 30, double, 3, 96, 4);
+    FFT3D_TWOPASS(30, 30, 30, double, 5, 160, 3);
     FFT3D_TWOPASS(45, 45, 45, float, 5, 256, 2);
     FFT3D_TWOPASS(45, 45, 45, float, 3, 160, 3);
     // 64^3: 64 = 8 x 8 staged lines, one plane or y-row per item

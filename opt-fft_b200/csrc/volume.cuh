@@ -119,6 +119,42 @@ FFT_HD cx<T> load_in(const cx<T> *p)
 #endif
 }
 
+// x lines of a prime length above 31 (47, 83 and 97 among the reference's test
+// extents): a folded sum held in registers would spill kilobytes a thread, so
+// the line is summed straight out of shared memory, one output at a time, with
+// double twiddles and accumulators; only x-pass lines are that long.
+constexpr bool x_direct_sum(int n) { return ce_is_prime(n) && n > 31; }
+
+template <class G, int S, bool KEEP>
+FFT_HD void pass_x_out_direct(const cx<typename G::T> *sm, int l, cx<typename G::T> *gout,
+                              typename G::T scale)
+{
+    using T = typename G::T;
+    constexpr int N = G::N0;
+    const int z = l % G::N2;
+    const int t = l / G::N2;
+    const int y = t % G::N1;
+    const int vol = t / G::N1;
+    cx<T> *o = gout + (long long)vol * G::V + y * G::N2 + z;
+    for (int k = 0; k < N; ++k) {
+        double ar = 0.0, ai = 0.0;
+        int e = 0;  // j * k mod N
+        for (int j = 0; j < N; ++j) {
+            const cx<T> x = sm[G::off((vol * N + j) * G::N1 + y, z)];
+            const auto w = line_tw<N, double>(e);  // {cos, sin}(2*pi*e/N)
+            const double sn = S > 0 ? w.y : -w.y;
+            ar += (double)x.re * w.x - (double)x.im * sn;
+            ai += (double)x.re * sn + (double)x.im * w.x;
+            e += k;
+            if (e >= N) e -= N;
+        }
+        cx<T> r = {(T)ar, (T)ai};
+        if constexpr (S > 0) r = cscale(r, scale);
+        if constexpr (KEEP) o[k * (G::N1 * G::N2)] = r;
+        else store_out(o + k * (G::N1 * G::N2), r);
+    }
+}
+
 // KEEP: plain stores instead of streaming (evict-first) ones, for outputs that
 // a following transform may still find in L2.
 template <class G, int S, int ALG, bool KEEP = false>
@@ -126,21 +162,25 @@ FFT_HD void pass_x_out(const cx<typename G::T> *sm, int l, cx<typename G::T> *go
                        typename G::T scale)
 {
     using T = typename G::T;
-    const int z = l % G::N2;
-    const int t = l / G::N2;
-    const int y = t % G::N1;
-    const int vol = t / G::N1;
-    cx<T> v[G::N0];
+    if constexpr (x_direct_sum(G::N0)) {
+        pass_x_out_direct<G, S, KEEP>(sm, l, gout, scale);
+    } else {
+        const int z = l % G::N2;
+        const int t = l / G::N2;
+        const int y = t % G::N1;
+        const int vol = t / G::N1;
+        cx<T> v[G::N0];
 #pragma unroll
-    for (int j = 0; j < G::N0; ++j) v[j] = sm[G::off((vol * G::N0 + j) * G::N1 + y, z)];
-    dft<G::N0, S, T, ALG>(v);
-    cx<T> *o = gout + (long long)vol * G::V + y * G::N2 + z;
+        for (int j = 0; j < G::N0; ++j) v[j] = sm[G::off((vol * G::N0 + j) * G::N1 + y, z)];
+        dft<G::N0, S, T, ALG>(v);
+        cx<T> *o = gout + (long long)vol * G::V + y * G::N2 + z;
 #pragma unroll
-    for (int j = 0; j < G::N0; ++j) {
-        cx<T> r = v[j];
-        if constexpr (S > 0) r = cscale(r, scale);
-        if constexpr (KEEP) o[j * (G::N1 * G::N2)] = r;
-        else store_out(o + j * (G::N1 * G::N2), r);
+        for (int j = 0; j < G::N0; ++j) {
+            cx<T> r = v[j];
+            if constexpr (S > 0) r = cscale(r, scale);
+            if constexpr (KEEP) o[j * (G::N1 * G::N2)] = r;
+            else store_out(o + j * (G::N1 * G::N2), r);
+        }
     }
 }
 

@@ -128,6 +128,60 @@ void register_kernels(std::vector<KernelEntry> &out)
     FFT3D_VOL(1, 8, 8, float, 0, 64, 512, 1);
     FFT3D_VOL(8, 1, 8, float, 0, 64, 512, 1);
     FFT3D_VOL(8, 8, 1, float, 0, 64, 512, 1);
+
+    // The rest of the reference's test geometries (python/test_fft3d.py:25-36):
+    // bare primes (5, 7, 11, and 19, 23, 47, 83, 97 along one axis -- folded
+    // direct sums; 83 and 97 spill, these are correctness extents), prime
+    // powers 25, 27, 49, unit and strongly anisotropic extents, 24x18x12 and
+    // 30^3 (complex64; the complex128 30^3 volume, 446 KB, runs as TWOPASS).
+    // About 48 KB of shared memory a CTA, lines of 32+ points on 256 threads.
+    FFT3D_VOL(2, 2, 2, double, 0, 64, 256, 1);
+    FFT3D_VOL(5, 5, 5, double, 0, 24, 512, 1);
+    FFT3D_VOL(7, 7, 7, double, 0, 8, 416, 1);
+    FFT3D_VOL(11, 11, 11, double, 0, 2, 256, 1);
+    FFT3D_VOL(49, 2, 2, double, 0, 10, 256, 1);
+    FFT3D_VOL(25, 4, 3, double, 0, 10, 512, 1);
+    FFT3D_VOL(27, 2, 2, double, 0, 18, 512, 1);
+    FFT3D_VOL(19, 3, 2, double, 0, 17, 512, 1);
+    FFT3D_VOL(23, 2, 2, double, 0, 22, 512, 1);
+    FFT3D_VOL(47, 3, 2, double, 0, 7, 256, 1);
+    FFT3D_VOL(83, 2, 1, double, 0, 18, 256, 1);
+    FFT3D_VOL(97, 2, 1, double, 0, 15, 256, 1);
+    FFT3D_VOL(1, 1, 16, double, 0, 64, 512, 1);
+    FFT3D_VOL(1, 7, 1, double, 0, 64, 448, 1);
+    FFT3D_VOL(3, 5, 7, double, 0, 29, 512, 1);
+    FFT3D_VOL(4, 6, 10, double, 0, 11, 512, 1);
+    FFT3D_VOL(16, 3, 5, double, 0, 12, 512, 1);
+    FFT3D_VOL(24, 18, 12, double, 0, 1, 448, 1);
+    FFT3D_VOL(2, 2, 64, double, 0, 12, 256, 1);
+    FFT3D_VOL(64, 2, 2, double, 0, 8, 256, 1);
+    FFT3D_VOL(9, 25, 7, double, 0, 1, 256, 1);
+    FFT3D_VOL(20, 12, 6, double, 0, 1, 256, 1);
+    FFT3D_VOL(11, 4, 9, double, 0, 7, 512, 1);
+    FFT3D_VOL(2, 2, 2, float, 0, 64, 256, 1);
+    FFT3D_VOL(5, 5, 5, float, 0, 49, 512, 1);
+    FFT3D_VOL(7, 7, 7, float, 0, 17, 512, 1);
+    FFT3D_VOL(11, 11, 11, float, 0, 4, 512, 1);
+    FFT3D_VOL(49, 2, 2, float, 0, 20, 256, 1);
+    FFT3D_VOL(25, 4, 3, float, 0, 20, 512, 1);
+    FFT3D_VOL(27, 2, 2, float, 0, 37, 512, 1);
+    FFT3D_VOL(19, 3, 2, float, 0, 35, 512, 1);
+    FFT3D_VOL(23, 2, 2, float, 0, 44, 512, 1);
+    FFT3D_VOL(47, 3, 2, float, 0, 14, 256, 1);
+    FFT3D_VOL(83, 2, 1, float, 0, 37, 256, 1);
+    FFT3D_VOL(97, 2, 1, float, 0, 31, 256, 1);
+    FFT3D_VOL(1, 1, 16, float, 0, 64, 512, 1);
+    FFT3D_VOL(1, 7, 1, float, 0, 64, 448, 1);
+    FFT3D_VOL(3, 5, 7, float, 0, 58, 512, 1);
+    FFT3D_VOL(4, 6, 10, float, 0, 23, 512, 1);
+    FFT3D_VOL(16, 3, 5, float, 0, 25, 512, 1);
+    FFT3D_VOL(24, 18, 12, float, 0, 1, 448, 1);
+    FFT3D_VOL(30, 30, 30, float, 0, 1, 512, 1);
+    FFT3D_VOL(2, 2, 64, float, 0, 24, 256, 1);
+    FFT3D_VOL(64, 2, 2, float, 0, 16, 256, 1);
+    FFT3D_VOL(9, 25, 7, float, 0, 3, 512, 1);
+    FFT3D_VOL(20, 12, 6, float, 0, 3, 512, 1);
+    FFT3D_VOL(11, 4, 9, float, 0, 15, 512, 1);
 }
 
 }  // namespace fft3d

@@ -1,9 +1,12 @@
 """Generate the golden vectors that pin the oracle and the CUDA path to the reference.
 
-Run in a checkout that has the reference's Python oracle (python/fft3d.py and
-python/slow_dft.py of wdetmold/opt-fft) at REF_ROOT (default /root/reference):
+Run with the reference's Python oracle (python/fft3d.py and python/slow_dft.py of
+wdetmold/opt-fft) in a checkout at PATH:
 
-    python tests/golden/make_golden.py [--ref-root PATH]
+    python tests/golden/make_golden.py --ref-root PATH [--missing]
+
+(--ref-root defaults to $REF_ROOT; one of them is required.  --missing writes
+only the fixtures that are not there yet.)
 
 It imports the reference's own code, transforms seeded inputs with it, and writes
 small .npz fixtures next to this script.  The fixtures are committed; the tests
@@ -52,6 +55,33 @@ CASES = [
     (1, (17, 2, 2), "normal", 120),
     (1, (3, 3, 3), "normal", 121),
     (1, (32, 8, 4), "normal", 122),
+    # the rest of python/test_fft3d.py:25-36
+    (2, (2, 2, 2), "normal", 123),
+    (1, (5, 5, 5), "normal", 124),
+    (1, (7, 7, 7), "normal", 125),
+    (1, (11, 11, 11), "normal", 126),
+    (1, (49, 2, 2), "normal", 127),
+    (1, (25, 4, 3), "normal", 128),
+    (1, (27, 2, 2), "normal", 129),
+    (1, (19, 3, 2), "normal", 130),
+    (1, (23, 2, 2), "normal", 131),
+    (1, (47, 3, 2), "normal", 132),
+    (1, (83, 2, 1), "normal", 133),
+    (1, (97, 2, 1), "normal", 134),
+    (1, (1, 1, 16), "normal", 135),
+    (1, (1, 7, 1), "normal", 136),
+    (1, (3, 5, 7), "normal", 137),
+    (1, (4, 6, 10), "normal", 138),
+    (1, (16, 3, 5), "normal", 139),
+    (1, (24, 18, 12), "normal", 140),
+    (1, (30, 30, 30), "normal", 141),
+    (1, (2, 2, 64), "normal", 142),
+    (1, (64, 2, 2), "normal", 143),
+    (1, (9, 25, 7), "normal", 144),
+    (1, (20, 12, 6), "normal", 145),
+    (1, (11, 4, 9), "normal", 146),
+    (1, (10, 10, 10), "normal", 147),
+    (1, (15, 15, 15), "normal", 148),
 ]
 
 
@@ -63,13 +93,19 @@ def field(rng, shape, dist):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref-root", default=os.environ.get("REF_ROOT", "/root/reference"))
+    ap.add_argument("--ref-root", default=os.environ.get("REF_ROOT"))
+    ap.add_argument("--missing", action="store_true", help="only write fixtures not present yet")
     a = ap.parse_args()
+    if not a.ref_root:
+        ap.error("--ref-root (or REF_ROOT) is required")
     sys.path.insert(0, os.path.join(a.ref_root, "python"))
     import fft3d  # noqa: E402  (the reference's textbook FFT)
     import slow_dft  # noqa: E402  (the reference's definitional DFT)
 
     for batch, shape, dist, seed in CASES:
+        name = "vol_%dx%dx%d_b%d.npz" % (shape + (batch,))
+        if a.missing and os.path.exists(os.path.join(HERE, name)):
+            continue
         rng = np.random.default_rng(seed)
         x = field(rng, (batch,) + shape, dist).astype(np.complex128)
         t0 = time.perf_counter()
@@ -78,11 +114,13 @@ def main():
         extra = {}
         if int(np.prod(shape)) <= 13 * 13 * 13:
             extra["sep"] = slow_dft.dft3d_separable(x)
-        name = "vol_%dx%dx%d_b%d.npz" % (shape + (batch,))
         np.savez_compressed(os.path.join(HERE, name), x=x, fwd=fwd, inv=inv,
                             shape=np.array(shape), seed=seed, dist=dist, **extra)
         print(f"{name}: {time.perf_counter() - t0:.2f}s")
 
+    if a.missing:
+        print("done")
+        return
     # complex64 contract: computed in double, returned as complex64 (fft3d.py:368-371)
     rng = np.random.default_rng(201)
     x32 = field(rng, (2, 8, 8, 8), "uniform").astype(np.complex64)

@@ -73,7 +73,7 @@ def test_invalid_descriptors_rejected_without_gpu_work():
             fb.Plan(shape, batch, direction, prec)
         assert e.value.status == fb.ERR_INVALID
     with pytest.raises(fb.Fft3dError) as e:
-        fb.Plan((7, 7, 7), 4)
+        fb.Plan((14, 14, 14), 4)
     assert e.value.status == fb.ERR_UNSUPPORTED
 
 

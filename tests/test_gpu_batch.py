@@ -145,7 +145,7 @@ def test_batch_rejects_bad_segments():
     y = torch.zeros_like(x)
     ok = {"shape": (8, 8, 8), "batch": 4, "in": x.data_ptr(), "out": y.data_ptr()}
     with pytest.raises(fb.Fft3dError) as e:
-        fb.Batch([dict(ok, shape=(7, 7, 7))])
+        fb.Batch([dict(ok, shape=(2, 2, 14))])  # no kernel for 14-point lines
     assert e.value.status == fb.ERR_UNSUPPORTED
     with pytest.raises(fb.Fft3dError) as e:
         fb.Batch([dict(ok, out=x.data_ptr() + 16)])

@@ -35,7 +35,10 @@ GEOMS = [(6, 6, 6), (8, 8, 8), (12, 12, 12), (16, 16, 16), (17, 17, 17), (24, 24
          # the other extents of the reference's tests (python/test_fft3d.py:25-36)
          (1, 1, 1), (3, 3, 3), (4, 4, 4), (9, 9, 9), (10, 10, 10), (15, 15, 15), (2, 3, 5),
          (7, 11, 13), (5, 8, 12), (13, 5, 8), (17, 2, 2), (32, 8, 4), (1, 8, 8), (8, 1, 8),
-         (8, 8, 1)]
+         (8, 8, 1), (2, 2, 2), (5, 5, 5), (7, 7, 7), (11, 11, 11), (49, 2, 2), (25, 4, 3),
+         (27, 2, 2), (19, 3, 2), (23, 2, 2), (47, 3, 2), (83, 2, 1), (97, 2, 1), (1, 1, 16),
+         (1, 7, 1), (3, 5, 7), (4, 6, 10), (16, 3, 5), (24, 18, 12), (30, 30, 30), (2, 2, 64),
+         (64, 2, 2), (9, 25, 7), (20, 12, 6), (11, 4, 9)]
 TDT = {fb.C128: torch.complex128, fb.C64: torch.complex64}
 NDT = {fb.C128: np.complex128, fb.C64: np.complex64}
 
@@ -109,8 +112,7 @@ GOLD = sorted(glob.glob(os.path.join(GOLDEN, "vol_*.npz")))
 def test_reference_golden_vectors(path):
     d = np.load(path)
     shape = tuple(int(s) for s in d["shape"])
-    if not fb.supports(shape, fb.C128):
-        pytest.skip(f"{shape} not compiled")
+    assert fb.supports(shape, fb.C128), f"{shape}: a reference test geometry without a kernel"
     x = d["x"]
     for direction, key in ((fb.FORWARD, "fwd"), (fb.BACKWARD, "inv")):
         plan = fb.Plan(shape, x.shape[0], direction, fb.C128)
@@ -168,7 +170,7 @@ def test_reference_device_abi_drop_in():
     torch.cuda.synchronize()
     assert oracle.rel_error_per_volume(dout.cpu().numpy(), oracle.fft3d(x)).max() < C128_TOL
     lib.fft3d_gpu_destroy(plan)
-    assert not lib.fft3d_gpu_create(7, 1)  # unsupported -> NULL (bench/gpu/fft3d_gpu_api.h:46-50)
+    assert not lib.fft3d_gpu_create(14, 1)  # unsupported -> NULL (bench/gpu/fft3d_gpu_api.h:46-50)
 
 
 def test_host_chain_round_trip_and_pinned_path():

@@ -117,9 +117,9 @@ def test_device_driver(tmp_path, L, batch):
 
 def test_device_driver_refuses_unsupported_size(tmp_path):
     drv = _driver("gpu_driver_b200")
-    x, inp = _input(tmp_path, 7, 2, seed=1)
+    x, inp = _input(tmp_path, 14, 2, seed=1)
     js = tmp_path / "r.json"
-    rc, log = _run([drv, "--L", 7, "--batch", 2, "--in", inp, "--json", js])
+    rc, log = _run([drv, "--L", 14, "--batch", 2, "--in", inp, "--json", js])
     assert rc == 3, log  # "not supported" is exit 3, not an error
     assert json.loads(open(js).read())["supported"] is False
 

@@ -145,7 +145,7 @@ def test_admission_budget_and_refusals():
         srv.submit({"shape": (36, 36, 36), "batch": 64, "in": big.data_ptr(), "out": bo.data_ptr()})
     assert e.value.status == fb.ERR_BUDGET
     with pytest.raises(fb.Fft3dError) as e:
-        srv.submit({"shape": (7, 7, 7), "batch": 1, "in": big.data_ptr(), "out": bo.data_ptr()})
+        srv.submit({"shape": (14, 14, 14), "batch": 1, "in": big.data_ptr(), "out": bo.data_ptr()})
     assert e.value.status == fb.ERR_UNSUPPORTED
     srv.close()
 

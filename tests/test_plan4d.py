@@ -50,7 +50,7 @@ def test_supports():
     assert lib.fft3d_b200_plan4d_supports(16, 8, 8, 8, fb.C128)
     assert lib.fft3d_b200_plan4d_supports(48, 24, 24, 24, fb.C64)
     assert not lib.fft3d_b200_plan4d_supports(7, 8, 8, 8, fb.C128)
-    assert not lib.fft3d_b200_plan4d_supports(16, 7, 7, 7, fb.C128)
+    assert not lib.fft3d_b200_plan4d_supports(16, 14, 14, 14, fb.C128)
 
 
 @pytest.mark.gpu

@@ -76,14 +76,18 @@ __device__ __forceinline__ void batch_passes(cx<typename G::T> *sm, int nv,
 
 // ---------------------------------------------------------------- two-phase large cube
 
-// One L^3 volume by one CTA: NS x-slabs of PL planes, then NS y-slabs of PL rows.
+// One L^3 volume by one CTA: NS x-slabs of PL planes through the z pass in
+// shared memory and the y pass, stored from registers into the CTA's scratch
+// volume (L2 only); then the x pass of all L*L lines straight out of scratch
+// into registers and on to the output -- no staging copy and no barrier in the
+// second phase.  The CTA barrier at the end of each slab orders its scratch
+// stores before the x pass's loads.
 template <int NT, int L, typename T, int S, int PL>
 __device__ __forceinline__ void big_cube(cx<T> *sm, const cx<T> *gin, cx<T> *gout, cx<T> *scratch, T scale)
 {
     constexpr int NS = L / PL;
     static_assert(NS * PL == L, "slabs of PL planes");
     using XG = Geom<PL, L, L, T>;  // x-slab: PL planes of L x L
-    using YG = Geom<L, PL, L, T>;  // y-slab: all x, PL rows of y
     const int tid = threadIdx.x;
     for (int s = 0; s < NS; ++s) {
         batch_load<NT, XG>(sm, gin + (long long)s * PL * L * L, PL * L * L);
@@ -91,31 +95,10 @@ __device__ __forceinline__ void big_cube(cx<T> *sm, const cx<T> *gin, cx<T> *gou
         __syncthreads();
         for (int r = tid; r < PL * L; r += NT) pass_z<XG, S, ALG_DEFAULT>(sm, r);
         __syncthreads();
-        for (int l = tid; l < PL * L; l += NT) pass_y<XG, S, ALG_DEFAULT>(sm, l);
-        __syncthreads();
-        cx<T> *dst = scratch + (long long)s * PL * L * L;
-        for (int g = tid; g < PL * L * L; g += NT) dst[g] = sm[XG::off(g / L, g % L)];
-        __syncthreads();
+        for (int l = tid; l < PL * L; l += NT) pass_y_store_l2<XG, S>(sm, l, scratch, s * PL);
+        __syncthreads();  // the slab's stores before the x pass; shared memory free again
     }
-    __threadfence();
-    __syncthreads();
-    for (int s = 0; s < NS; ++s) {
-        // rows (x, y - s*PL) of the y-slab; the source rows are L*L apart in scratch
-        for (int g = tid; g < L * PL * L; g += NT) {
-            const int z = g % L;
-            const int row = g / L;  // x * PL + yl
-            const int x = row / PL, yl = row % PL;
-            cx<T> *d = sm + YG::off(row, z);
-            const cx<T> *src = scratch + ((long long)x * L + s * PL + yl) * L + z;
-            if constexpr (sizeof(T) == 8) cp_async_16(d, src);
-            else cp_async_8(d, src);
-        }
-        cp_async_commit();
-        cp_async_wait<0>();
-        __syncthreads();
-        for (int l = tid; l < PL * L; l += NT) pass_x_slab<YG, S, L>(sm, l, gout, s * PL, scale);
-        __syncthreads();
-    }
+    for (int l = tid; l < L * L; l += NT) pass_x_load_l2<L, L, L, S, T>(scratch, l, gout, 0, scale);
 }
 
 // ---------------------------------------------------------------- dispatch

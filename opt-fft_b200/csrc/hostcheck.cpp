@@ -82,18 +82,17 @@ static void emulate_cluster(const void *vin, void *vout, long long nvol)
     }
 }
 
-// The batch kernel's two-phase cube: x-slabs (z, y passes) to scratch, then
-// y-slabs from scratch through the x pass (batch_kernel.cu big_cube).
+// The batch kernel's two-phase cube: x-slabs (z pass, y pass stored to scratch), then
+// the x pass of every line straight out of scratch (batch_kernel.cu big_cube).
 template <int L, typename T, int S, int PL>
 static void emulate_big_cube(const void *vin, void *vout, long long nvol)
 {
     constexpr int NS = L / PL;
     using XG = Geom<PL, L, L, T>;
-    using YG = Geom<L, PL, L, T>;
     constexpr long long V = (long long)L * L * L;
     const T scale = S > 0 ? T(1) / T(V) : T(1);
-    std::vector<cx<T>> sm((size_t)(XG::PV > YG::PV ? XG::PV : YG::PV));
-    std::vector<cx<T>> scratch((size_t)V);
+    std::vector<cx<T>> sm((size_t)XG::PV);
+    std::vector<cx<T>> scratch((size_t)V, cx<T>{T(-777.0), T(555.0)});
     for (long long vol = 0; vol < nvol; ++vol) {
         const cx<T> *gin = (const cx<T> *)vin + vol * V;
         cx<T> *gout = (cx<T> *)vout + vol * V;
@@ -102,18 +101,9 @@ static void emulate_big_cube(const void *vin, void *vout, long long nvol)
             for (int g = 0; g < PL * L * L; ++g)
                 sm[XG::off(g / L, g % L)] = gin[(long long)s * PL * L * L + g];
             for (int r = 0; r < PL * L; ++r) pass_z<XG, S, ALG_DEFAULT>(sm.data(), r);
-            for (int l = 0; l < PL * L; ++l) pass_y<XG, S, ALG_DEFAULT>(sm.data(), l);
-            for (int g = 0; g < PL * L * L; ++g)
-                scratch[(size_t)s * PL * L * L + g] = sm[XG::off(g / L, g % L)];
+            for (int l = 0; l < PL * L; ++l) pass_y_store_l2<XG, S>(sm.data(), l, scratch.data(), s * PL);
         }
-        for (int s = 0; s < NS; ++s) {
-            for (auto &e : sm) e = {T(12345.0), T(-6789.0)};
-            for (int g = 0; g < L * PL * L; ++g) {
-                const int z = g % L, row = g / L, x = row / PL, yl = row % PL;
-                sm[YG::off(row, z)] = scratch[((size_t)x * L + s * PL + yl) * L + z];
-            }
-            for (int l = 0; l < PL * L; ++l) pass_x_slab<YG, S, L>(sm.data(), l, gout, s * PL, scale);
-        }
+        for (int l = 0; l < L * L; ++l) pass_x_load_l2<L, L, L, S, T>(scratch.data(), l, gout, 0, scale);
     }
 }
 

@@ -34,7 +34,7 @@ struct KindInfo {
 template <int N0, int N1, int N2, typename T, int VPC, int BIG>
 constexpr long long kind_stage_bytes()
 {
-    if constexpr (BIG > 0) return (long long)Geom<BIG, N1, N2, T>::PV * Geom<BIG, N1, N2, T>::EB;
+    if constexpr (BIG > 0) return 2LL * Geom<BIG, N1, N2, T>::PV * Geom<BIG, N1, N2, T>::EB;  // two slab buffers
     else return (long long)VPC * Geom<N0, N1, N2, T>::PV * Geom<N0, N1, N2, T>::EB;
 }
 

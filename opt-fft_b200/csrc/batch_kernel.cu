@@ -80,8 +80,9 @@ __device__ __forceinline__ void batch_passes(cx<typename G::T> *sm, int nv,
 // shared memory and the y pass, stored from registers into the CTA's scratch
 // volume (L2 only); then the x pass of all L*L lines straight out of scratch
 // into registers and on to the output -- no staging copy and no barrier in the
-// second phase.  The CTA barrier at the end of each slab orders its scratch
-// stores before the x pass's loads.
+// second phase.  The slabs are double-buffered: the next slab's planes load
+// while the current one is transformed.  The CTA barrier at the end of each
+// slab orders its scratch stores before the x pass's loads.
 template <int NT, int L, typename T, int S, int PL>
 __device__ __forceinline__ void big_cube(cx<T> *sm, const cx<T> *gin, cx<T> *gout, cx<T> *scratch, T scale)
 {
@@ -89,14 +90,20 @@ __device__ __forceinline__ void big_cube(cx<T> *sm, const cx<T> *gin, cx<T> *gou
     static_assert(NS * PL == L, "slabs of PL planes");
     using XG = Geom<PL, L, L, T>;  // x-slab: PL planes of L x L
     const int tid = threadIdx.x;
+    batch_load<NT, XG>(sm, gin, PL * L * L);
     for (int s = 0; s < NS; ++s) {
-        batch_load<NT, XG>(sm, gin + (long long)s * PL * L * L, PL * L * L);
-        cp_async_wait<0>();
+        cx<T> *buf = sm + (s & 1) * XG::PV;
+        if (s + 1 < NS) {
+            batch_load<NT, XG>(sm + ((s + 1) & 1) * XG::PV, gin + (long long)(s + 1) * PL * L * L, PL * L * L);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
         __syncthreads();
-        for (int r = tid; r < PL * L; r += NT) pass_z<XG, S, ALG_DEFAULT>(sm, r);
+        for (int r = tid; r < PL * L; r += NT) pass_z<XG, S, ALG_DEFAULT>(buf, r);
         __syncthreads();
-        for (int l = tid; l < PL * L; l += NT) pass_y_store_l2<XG, S>(sm, l, scratch, s * PL);
-        __syncthreads();  // the slab's stores before the x pass; shared memory free again
+        for (int l = tid; l < PL * L; l += NT) pass_y_store_l2<XG, S>(buf, l, scratch, s * PL);
+        __syncthreads();  // the slab's stores before the x pass; its buffer free again
     }
     for (int l = tid; l < L * L; l += NT) pass_x_load_l2<L, L, L, S, T>(scratch, l, gout, 0, scale);
 }

@@ -28,6 +28,7 @@ struct BatchSeg {
 // X(id, n0, n1, n2, real type, sign, volumes per item, solo, big-cube slab planes)
 //   solo: the item needs all of shared memory (no prefetch around it)
 //   big:  0, or the slab thickness of the two-phase path for cubes beyond one SM
+//         (two slab buffers in shared memory)
 #define FFT3D_BATCH_KINDS(X)                         \
     X(0, 6, 6, 6, double, -1, 28, 0, 0)              \
     X(1, 6, 6, 6, double, +1, 28, 0, 0)              \
@@ -41,8 +42,8 @@ struct BatchSeg {
     X(9, 17, 17, 17, double, +1, 1, 0, 0)            \
     X(10, 24, 24, 24, double, -1, 1, 1, 0)           \
     X(11, 24, 24, 24, double, +1, 1, 1, 0)           \
-    X(12, 36, 36, 36, double, -1, 1, 1, 9)           \
-    X(13, 36, 36, 36, double, +1, 1, 1, 9)           \
+    X(12, 36, 36, 36, double, -1, 1, 1, 4)           \
+    X(13, 36, 36, 36, double, +1, 1, 1, 4)           \
     X(14, 8, 8, 16, double, -1, 7, 0, 0)             \
     X(15, 8, 8, 16, double, +1, 7, 0, 0)             \
     X(16, 16, 16, 32, double, -1, 1, 1, 0)           \
@@ -59,8 +60,8 @@ struct BatchSeg {
     X(27, 17, 17, 17, float, +1, 2, 0, 0)            \
     X(28, 24, 24, 24, float, -1, 1, 0, 0)            \
     X(29, 24, 24, 24, float, +1, 1, 0, 0)            \
-    X(30, 36, 36, 36, float, -1, 1, 1, 12)           \
-    X(31, 36, 36, 36, float, +1, 1, 1, 12)           \
+    X(30, 36, 36, 36, float, -1, 1, 1, 6)            \
+    X(31, 36, 36, 36, float, +1, 1, 1, 6)            \
     X(32, 8, 8, 16, float, -1, 14, 0, 0)              \
     X(33, 8, 8, 16, float, +1, 14, 0, 0)              \
     X(34, 16, 16, 32, float, -1, 1, 0, 0)            \
@@ -84,8 +85,8 @@ constexpr int BATCH_NKINDS = 36;
     X(27, 17, 17, 17, float, +1, 1, 0, 0)            \
     X(28, 24, 24, 24, float, -1, 1, 1, 0)            \
     X(29, 24, 24, 24, float, +1, 1, 1, 0)            \
-    X(30, 36, 36, 36, float, -1, 1, 1, 9)            \
-    X(31, 36, 36, 36, float, +1, 1, 1, 9)            \
+    X(30, 36, 36, 36, float, -1, 1, 1, 4)            \
+    X(31, 36, 36, 36, float, +1, 1, 1, 4)            \
     X(32, 8, 8, 16, float, -1, 7, 0, 0)              \
     X(33, 8, 8, 16, float, +1, 7, 0, 0)              \
     X(34, 16, 16, 32, float, -1, 1, 1, 0)            \

@@ -418,7 +418,7 @@ static const EmuEntry kEmu[] = {
     EMU(1, 1, 1, double, 0, 1),    EMU(3, 3, 3, double, 0, 1),     EMU(17, 2, 2, double, 0, 1),
     EMU_CL(36, 36, 36, double, 4), EMU_CL(36, 36, 36, double, 6),  EMU_CL(36, 36, 36, double, 9),
     EMU_CL(36, 36, 36, float, 2),  EMU_CL(36, 36, 36, float, 4),   EMU_CL(36, 36, 36, float, 6),
-    EMU_BIG(36, double, 9),        EMU_BIG(36, float, 12),  EMU_BIG(36, float, 9),
+    EMU_BIG(36, double, 4),        EMU_BIG(36, float, 6),   EMU_BIG(36, float, 4),
     EMU_TP(36, 36, 36, double, 4), EMU_TP(36, 36, 36, double, 2),  EMU_TP(36, 36, 36, double, 6),
     EMU_TP(36, 36, 36, float, 4),  EMU_TP(36, 36, 36, float, 6),   EMU_TP(16, 16, 32, double, 4),
     EMU_TP(16, 16, 32, double, 8), EMU_TP(6, 9, 5, double, 3),     EMU_TP(36, 36, 36, double, 3),

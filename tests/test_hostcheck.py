@@ -105,7 +105,7 @@ def test_cluster_data_movement(hostcheck, prec, c, sign):
     assert err < (C128_TOL if prec == 0 else C64_TOL), err
 
 
-@pytest.mark.parametrize("n,prec,pl", [(36, 0, 9), (36, 1, 12), (36, 1, 9)])
+@pytest.mark.parametrize("n,prec,pl", [(36, 0, 4), (36, 1, 6), (36, 1, 4)])
 @pytest.mark.parametrize("sign", [-1, +1])
 def test_two_phase_cube(hostcheck, n, prec, pl, sign):
     """The batch kernel's two-phase route through scratch (alg = 200 + slab

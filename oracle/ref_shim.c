@@ -16,7 +16,12 @@
  *                 bench/geom/sota/fftw3.c:43-48 with its planner flags;
  *   REF_FFTW_THREADS  one fftw_plan_many_dft over the whole batch planned with
  *                 fftw_plan_with_nthreads(nthreads), as bench/mt/sota/fftw3.c:37-48
- *                 does with its fixed 32 threads.
+ *                 does with its fixed 32 threads;
+ *   REF_MT        one of the reference's multicore kernels (bench/mt/impl_4/L*.c,
+ *                 the six symbols of bench/mt/fft3d_api.h, built one shared object
+ *                 each and opened by ref_open_mt): one plan over the whole batch,
+ *                 its own OpenMP threads, their count set as the reference's
+ *                 harness fixes OMP_NUM_THREADS (bench/mt/fft3d_api.h "MULTICORE").
  * This file adds only the thread pool (workers created once, released by a
  * barrier for every run, so a timed run pays no thread creation), the slicing,
  * and the inverse half of a round trip: FFTW_BACKWARD plans and a 1/V scale for
@@ -24,7 +29,9 @@
  * ifft(X) = conj(fft(conj(X))) / V.
  */
 #include <complex.h>
+#include <dlfcn.h>
 #include <fftw3.h>
+#include <omp.h>
 #include <pthread.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -64,7 +71,16 @@ tb_plan *tb_create(int L, int batch);
 void tb_execute(tb_plan *p, const cplx *in, cplx *out);
 void tb_destroy(tb_plan *p);
 
-enum { REF_BEST = 0, REF_TEXTBOOK = 1, REF_FFTW = 2, REF_FFTW_THREADS = 3 };
+enum { REF_BEST = 0, REF_TEXTBOOK = 1, REF_FFTW = 2, REF_FFTW_THREADS = 3, REF_MT = 4 };
+
+/* a bench/mt kernel opened by ref_open_mt */
+struct mt_kernel {
+    const char *(*name)(void);
+    int (*supports)(int);
+    void *(*create)(int, int);
+    void (*execute)(void *, const cplx *, cplx *);
+    void (*destroy)(void *);
+};
 #define MAXT 512
 
 struct slice {
@@ -95,6 +111,9 @@ typedef struct ref_ctx {
     int quit;
     double plan_seconds;
     char name[160];
+    struct mt_kernel mt;        /* REF_MT */
+    void *mt_plan;
+    int omp_threads;
 } ref_ctx;
 
 static double now_s(void)
@@ -368,11 +387,64 @@ ref_ctx *ref_create(int L, long batch, int nthreads, int roundtrip)
     return ref_open(REF_BEST, L, L, L, batch, 0, nthreads, roundtrip, 0);
 }
 
+/* A bench/mt/impl_4 kernel from its shared object, with `nthreads` OpenMP
+ * threads (complex128 cubes), one plan over the whole batch.  The kernels are
+ * forward-only and tuned for whole large batches (their per-call overhead makes
+ * any chunked inverse unfair to them), so a "round trip" here is charged as two
+ * forward transforms of the batch, in -> tmp -> out: the cost of a round trip
+ * whose inverse ran as fast as the forward, with no conjugation or scaling;
+ * out is then FFT(FFT(in)) = V times the index reversal of in.  The object
+ * stays loaded for the life of the process. */
+ref_ctx *ref_open_mt(const char *path, int L, long batch, int nthreads, int roundtrip)
+{
+    if (!path || L < 1 || batch < 1 || batch > 0x7fffffffL || nthreads < 1) return NULL;
+    void *h = dlopen(path, RTLD_NOW | RTLD_LOCAL);
+    if (!h) return NULL;
+    ref_ctx *c = calloc(1, sizeof *c);
+    if (!c) return NULL;
+    c->mt.name = (const char *(*)(void))dlsym(h, "fft3d_name");
+    c->mt.supports = (int (*)(int))dlsym(h, "fft3d_supports");
+    c->mt.create = (void *(*)(int, int))dlsym(h, "fft3d_create");
+    c->mt.execute = (void (*)(void *, const cplx *, cplx *))dlsym(h, "fft3d_execute");
+    c->mt.destroy = (void (*)(void *))dlsym(h, "fft3d_destroy");
+    if (!c->mt.name || !c->mt.supports || !c->mt.create || !c->mt.execute || !c->mt.destroy ||
+        !c->mt.supports(L))
+        goto fail;
+    c->backend = REF_MT;
+    c->n0 = c->n1 = c->n2 = L;
+    c->roundtrip = roundtrip;
+    c->batch = batch;
+    c->vol = (long)L * L * L;
+    c->nthreads = 1;  /* no pool: the kernel runs its own threads */
+    c->omp_threads = nthreads;
+    omp_set_num_threads(nthreads);
+    const double t0 = now_s();
+    c->mt_plan = c->mt.create(L, (int)batch);
+    if (!c->mt_plan) goto fail;
+    if (roundtrip && posix_memalign(&c->tmp, 64, (size_t)batch * c->vol * sizeof(cplx))) goto fail;
+    c->plan_seconds = now_s() - t0;
+    snprintf(c->name, sizeof c->name, "bench/mt/impl_4 %s (OpenMP, %d threads)", c->mt.name(), nthreads);
+    return c;
+fail:
+    free(c);
+    return NULL;
+}
+
 int ref_run(ref_ctx *c, const void *in, void *out)
 {
     if (!c) return -1;
     c->in = in;
     c->out = out;
+    if (c->backend == REF_MT) {
+        omp_set_num_threads(c->omp_threads);
+        if (!c->roundtrip) {
+            c->mt.execute(c->mt_plan, (const cplx *)in, (cplx *)out);
+        } else {
+            c->mt.execute(c->mt_plan, (const cplx *)in, (cplx *)c->tmp);
+            c->mt.execute(c->mt_plan, (const cplx *)c->tmp, (cplx *)out);
+        }
+        return 0;
+    }
     if (c->backend != REF_FFTW_THREADS) {
         pool_run(c, job_slice);
         return 0;
@@ -397,12 +469,18 @@ int ref_run(ref_ctx *c, const void *in, void *out)
 }
 
 const char *ref_kernel_name(ref_ctx *c) { return c ? c->name : ""; }
-int ref_threads(ref_ctx *c) { return c ? c->nthreads : 0; }
+int ref_threads(ref_ctx *c) { return c ? (c->backend == REF_MT ? c->omp_threads : c->nthreads) : 0; }
 double ref_plan_seconds(ref_ctx *c) { return c ? c->plan_seconds : 0.0; }
 
 void ref_destroy(ref_ctx *c)
 {
     if (!c) return;
+    if (c->backend == REF_MT) {
+        if (c->mt_plan) c->mt.destroy(c->mt_plan);
+        free(c->tmp);
+        free(c);
+        return;
+    }
     if (c->nthreads > 1) {
         c->quit = 1;
         pthread_barrier_wait(&c->start);

@@ -89,3 +89,48 @@ def test_unsupported_requests_are_refused():
     assert not lib.ref_open(BEST, 7, 7, 7, 4, 0, 1, 0, 0)       # no best kernel for 7
     assert not lib.ref_open(BEST, 8, 8, 16, 4, 0, 1, 0, 0)      # cubes only
     assert not lib.ref_open(TEXTBOOK, 8, 8, 8, 4, 1, 1, 0, 0)   # complex double only
+
+
+MT = sorted(__import__("glob").glob(os.path.join(ROOT, "oracle", "_ref", "mt", "L*.so")))
+
+
+@pytest.mark.parametrize("path", [p for p in MT if os.path.basename(p).startswith(("L6_", "L8_", "L13_"))],
+                         ids=lambda p: os.path.basename(p))
+@pytest.mark.parametrize("roundtrip", [False, True])
+def test_multicore_kernels_match_oracle(path, roundtrip):
+    """The reference's multicore kernels (bench/mt/impl_4, one shared object
+    each, opened by ref_open_mt): forward against the oracle; the "round trip"
+    the bench charges them (two forward transforms) against its known answer,
+    FFT(FFT(x)) = V times the index reversal of x."""
+    lib = _lib()
+    lib.ref_open_mt.restype = ctypes.c_void_p
+    lib.ref_open_mt.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_long, ctypes.c_int, ctypes.c_int]
+    L = int(os.path.basename(path).split("_")[0][1:])
+    batch = 5
+    x = aligned((batch, L, L, L), np.complex128)
+    x[...] = field(np.random.default_rng(L + batch), (batch, L, L, L))
+    out = aligned((batch, L, L, L), np.complex128)
+    ctx = lib.ref_open_mt(path.encode(), L, batch, 2, 1 if roundtrip else 0)
+    assert ctx, path
+    try:
+        assert lib.ref_threads(ctx) == 2
+        lib.ref_run(ctx, x.ctypes.data, out.ctypes.data)
+        assert "bench/mt/impl_4" in lib.ref_kernel_name(ctx).decode()
+    finally:
+        lib.ref_destroy(ctx)
+    if roundtrip:
+        want = L ** 3 * np.roll(x[:, ::-1, ::-1, ::-1], 1, axis=(1, 2, 3))  # x[b, -i, -j, -k]
+    else:
+        want = oracle.fft3d(x)
+    assert oracle.rel_error(out, want) < 1e-12
+
+
+def test_multicore_kernel_refuses_other_sizes():
+    lib = _lib()
+    lib.ref_open_mt.restype = ctypes.c_void_p
+    lib.ref_open_mt.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_long, ctypes.c_int, ctypes.c_int]
+    p8 = [p for p in MT if os.path.basename(p).startswith("L8_")]
+    if not p8:
+        pytest.skip("no L=8 multicore kernel built")
+    assert not lib.ref_open_mt(p8[0].encode(), 9, 4, 2, 0)
+    assert not lib.ref_open_mt(b"/nonexistent.so", 8, 4, 2, 0)

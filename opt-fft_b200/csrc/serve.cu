@@ -93,6 +93,7 @@ struct fft3d_b200_server {
     std::mutex mu;
     std::condition_variable cv;
     std::deque<ServeReq> pending;
+    std::atomic<long long> npending{0};  // pending.size(), readable without the lock
     std::deque<unsigned long long> completed;
     unsigned long long next_ticket = 1;
     unsigned long long submitted = 0, finished = 0;
@@ -222,9 +223,31 @@ static void server_loop(fft3d_b200_server *s)
     cudaSetDevice(s->device);
     const bool plain = (s->flags & FFT3D_B200_SERVE_PLAIN) != 0;
     std::vector<ServeSlot *> to_launch;
+    bool blocked = false;  // the queue's head waits for a slot or for budget
     while (true) {
+        // Without the lock (only this thread changes the slots): is there work --
+        // a launch that finished, or a request that may be admitted?  While
+        // launches are in flight the thread polls (a sleep would round up to
+        // the kernel's timer slack, tens of microseconds); idle, it waits for a
+        // submission.  Submitters take the lock only to queue.
+        bool in_flight = false, finished = false;
+        for (ServeSlot &slot : s->slots) {
+            if (!slot.busy) continue;
+            in_flight = true;
+            if (!finished && cudaEventQuery(slot.done) != cudaErrorNotReady) finished = true;
+        }
+        const bool admissible = !blocked && s->npending.load(std::memory_order_acquire) > 0;
+        if (!finished && !admissible && !s->stop.load()) {
+            if (in_flight) {
+                std::this_thread::yield();
+            } else {
+                std::unique_lock<std::mutex> lk(s->mu);
+                if (s->pending.empty() && !s->stop) s->cv.wait_for(lk, std::chrono::milliseconds(1));
+                blocked = false;
+            }
+            continue;
+        }
         std::unique_lock<std::mutex> lk(s->mu);
-        bool progress = false;
         // retire finished launches
         for (ServeSlot &slot : s->slots) {
             if (!slot.busy) continue;
@@ -244,7 +267,6 @@ static void server_loop(fft3d_b200_server *s)
             slot.reqs.clear();
             slot.bytes = 0;
             slot.busy = false;
-            progress = true;
         }
         // admit pending requests, FIFO, into free slots
         to_launch.clear();
@@ -263,6 +285,7 @@ static void server_loop(fft3d_b200_server *s)
                 slot.bytes += r.bytes;
                 slot.reqs.push_back(r);
                 s->pending.pop_front();
+                s->npending.fetch_sub(1, std::memory_order_relaxed);
             }
             if (slot.reqs.empty()) break;  // head of queue waits for budget
             s->peak_used = std::max(s->peak_used, s->used);
@@ -270,17 +293,13 @@ static void server_loop(fft3d_b200_server *s)
             ++s->batches;
             s->batched_requests += (long long)slot.reqs.size();
             to_launch.push_back(&slot);
-            progress = true;
         }
+        // requests left queued wait for a launch to finish (a slot or budget)
+        blocked = !s->pending.empty();
         s->cv.notify_all();
         bool any_busy = false;
         for (const ServeSlot &slot : s->slots) any_busy |= slot.busy;
         if (s->stop && s->pending.empty() && !any_busy) break;
-        if (!progress && !any_busy) {
-            // idle: wait for a submission
-            s->cv.wait_for(lk, std::chrono::milliseconds(1));
-            continue;
-        }
         // descriptors and launches outside the lock: submitters are not held up;
         // the slots are this thread's own until they are retired above
         lk.unlock();
@@ -291,7 +310,6 @@ static void server_loop(fft3d_b200_server *s)
                 s->status = st;
             }
         }
-        if (!progress) std::this_thread::sleep_for(std::chrono::microseconds(5));
     }
 }
 
@@ -410,6 +428,7 @@ static int server_submit_at(fft3d_b200_server *s, const fft3d_b200_segment *req,
         if (s->submitted == 0) s->t_first = r.t_submit;
         ++s->submitted;
         s->pending.push_back(r);
+        s->npending.fetch_add(1, std::memory_order_release);
     }
     s->cv.notify_all();
     if (ticket) *ticket = r.ticket;

@@ -448,7 +448,8 @@ def measure_serve(fb, torch, device, n_req=1_000_000, seed=2024, arena_gb=(24, 4
     requests in complex128.  Runs: saturation (everything queued at once), then
     Poisson arrivals at 70% of the batched saturation rate; the baseline at that
     same rate and at 70% of its own saturation rate.  p50/p99 are taken over the
-    steady-state window (requests 1%..99% of the stream by submission order)."""
+    steady-state window (requests 1%..99% of the stream by submission order); the
+    batched Poisson stream runs three times and reports its median-p99 run."""
     from fft3d_b200.workloads import SIDES, arena_offsets, request_arrays
     ra = request_arrays(n_req, rate_hz=1.0, seed=seed)
     side, nvol = ra["side"], ra["batch"]
@@ -537,7 +538,12 @@ def measure_serve(fb, torch, device, n_req=1_000_000, seed=2024, arena_gb=(24, 4
     sat = run(0, None, False, 4)
     lam = 0.7 * sat["requests_per_s"]
     out["batched_saturation"] = sat
-    out["batched_poisson"] = run(0, lam, False, 4)
+    # the headline latency: three runs of the same seeded stream, the run with
+    # the median p99 reported (host scheduling moves the tail from run to run)
+    runs = sorted((run(0, lam, False, 4) for _ in range(3)), key=lambda r: r["p99_s"])
+    runs[1]["p99_runs_s"] = [r["p99_s"] for r in runs]
+    runs[1]["p50_runs_s"] = [r["p50_s"] for r in runs]
+    out["batched_poisson"] = runs[1]
     psat = run(fb.SERVE_PLAIN, None, True, 32)
     out["plain_fp64_saturation"] = psat
     out["plain_fp64_poisson_same_rate"] = run(fb.SERVE_PLAIN, lam, True, 32)

@@ -30,6 +30,7 @@ import argparse
 import ctypes
 import glob
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -880,6 +881,15 @@ def measure_cufft(torch, wl, stream, steps, warmup, peak):
 
 # ------------------------------------------------------------------ main
 
+def gflops(name, volumes_per_s):
+    """Nominal GF/s: 5 N log2 N flops per 3D transform of N = n0 n1 n2 points, times
+    the transforms of a step per volume (bench/geom/driver.c:255-260's yardstick;
+    not the kernels' real operation count)."""
+    w = WORKLOADS[name]
+    n = float(np.prod(w["shape"]))
+    return volumes_per_s * len(w["chain"]) * 5.0 * n * math.log2(n) / 1e9 if n > 1 else 0.0
+
+
 def make_config(name, world, nsets=None):
     """The config block both arms report, so that they compare like with like."""
     w = WORKLOADS[name]
@@ -941,6 +951,7 @@ def reference_arm(a, world, rank, metric):
             f"threads, planned once ({r['plan_s']:.1f} s, untimed), in a child process; chosen by a 3-run "
             f"race of {'; '.join(race)}")
     line = {"impl": "reference", "metric": metric, "value": value, "unit": "volumes/s",
+            "gflops_nominal": gflops(a.workload, value),
             "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": per * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if w["prec"] == 0 else "f32", "data": "synthetic",
@@ -1021,7 +1032,8 @@ def main():
     e2e = None
     if not a.no_e2e:
         e2e_s, h2d, d2h = time_e2e(fb, torch, wl, max(3, min(50, a.steps // 4)), 2, dist)
-        e2e = {"value": world * wl.batch / e2e_s, "unit": "volumes/s", "h2d_bytes_per_step": h2d,
+        e2e = {"value": world * wl.batch / e2e_s, "unit": "volumes/s",
+               "gflops_nominal": gflops(a.workload, world * wl.batch / e2e_s), "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h,
                "path": "fft3d_b200_execute_host_chain, page-locked host buffers"}
         if world == 1:
@@ -1055,6 +1067,7 @@ def main():
             ach = ab / (f * 1e-3) / 1e9
             cfx = copy_floor(torch, x, stream, max(5, a.steps // 2), a.warmup)
             workloads[name] = {"label": ww["label"], "volumes_per_s": world * x.batch / (m * 1e-3),
+                               "gflops_nominal": gflops(name, world * x.batch / (m * 1e-3)),
                                "ms_per_launch": f, "achieved_gbs": ach, "frac": ach / peak,
                                "copy_same_bytes_gbs": cfx, "frac_of_copy_same_bytes": ach / cfx,
                                "kernel": x.plans[0].describe(),
@@ -1113,6 +1126,7 @@ def main():
                           "plain_fp64_p99_s": serve["plain_fp64_poisson_own_rate"]["p99_s"],
                           "n_requests": serve["n_requests"]}
     line = {"metric": metric, "value": value, "unit": "volumes/s", "n_gpus": world,
+            "gflops_nominal": gflops(a.workload, value),
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if w["prec"] == 0 else "f32",
             "data": "synthetic", "config": make_config(a.workload, world),

@@ -184,3 +184,48 @@ def test_extents_outside_the_batch_kinds():
     for s, p, d, x, xi, xo in work:
         err = oracle.rel_error_per_volume(xo.cpu().numpy().astype(np.complex128), ref(x, d))
         assert err.max() < (C128_TOL if p == fb.C128 else C64_TOL), (s, p, d, err.max())
+
+
+def test_concurrent_submitters():
+    """fft3d_b200_server_submit is thread-safe: four host threads submit at
+    once (mixed extents, directions and precisions, some with no batch kind);
+    every ticket completes exactly once and every result matches the oracle."""
+    import threading
+    rng = np.random.default_rng(21)
+    shapes = [(8, 8, 8), (17, 17, 17), (12, 12, 12), (9, 9, 9), (6, 6, 6), (16, 16, 32)]
+    work = []
+    for k in range(48):
+        shape = shapes[k % len(shapes)]
+        prec = fb.C128 if k % 3 else fb.C64
+        d = fb.FORWARD if k % 2 else fb.BACKWARD
+        dt = np.complex128 if prec == fb.C128 else np.complex64
+        x = field(rng, (1 + k % 5,) + shape, "uniform", dt)
+        xi = torch.from_numpy(x).cuda()
+        work.append((shape, prec, d, x, xi, torch.full_like(xi, complex(3.0, 3.0))))
+    srv = fb.Server(budget_bytes=8 << 30, max_inflight=3)
+    tickets = [None] * len(work)
+
+    def submit(part):
+        for i in range(part, len(work), 4):
+            s, p, d, x, xi, xo = work[i]
+            tickets[i] = srv.submit({"shape": s, "batch": x.shape[0], "direction": d, "precision": p,
+                                     "in": xi.data_ptr(), "out": xo.data_ptr()})
+
+    threads = [threading.Thread(target=submit, args=(t,)) for t in range(4)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    srv.drain(60)
+    done = []
+    while True:
+        got = srv.poll()
+        if not got:
+            break
+        done += got
+    assert sorted(done) == sorted(tickets) and len(set(tickets)) == len(work)
+    srv.close()
+    torch.cuda.synchronize()
+    for s, p, d, x, xi, xo in work:
+        err = oracle.rel_error_per_volume(xo.cpu().numpy().astype(np.complex128), ref(x, d))
+        assert err.max() < (C128_TOL if p == fb.C128 else C64_TOL), (s, p, d, err.max())

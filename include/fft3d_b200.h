@@ -260,9 +260,10 @@ int fft3d_b200_server_create(size_t hbm_budget_bytes, int max_inflight, unsigned
 /* Queue one request (thread-safe).  FFT3D_B200_ERR_BUDGET if it alone exceeds
  * the budget.  `ticket` identifies it in fft3d_b200_server_poll.  Extents of the
  * persistent batch kernel are coalesced; any other extent with a kernel that
- * needs no plan workspace is served by its own launch in the same slot, and
- * the rest (45^3, 64^3, complex128 30^3: kernels with a scratch ring) are
- * refused with FFT3D_B200_ERR_UNSUPPORTED. */
+ * compiled extent is served by its own tuned launch in the same slot (a
+ * kernel with a scratch ring -- 45^3, 64^3, complex128 30^3 -- with the slot's
+ * workspace, allocated on first need); an extent without a kernel is refused
+ * with FFT3D_B200_ERR_UNSUPPORTED. */
 int fft3d_b200_server_submit(fft3d_b200_server *server, const fft3d_b200_segment *request,
                              unsigned long long *ticket);
 

@@ -87,12 +87,13 @@ int entry_occupancy(const KernelEntry &e, int device);
 
 int element_bytes(int precision);
 
-// Whether a geometry has a kernel that needs no plan workspace (what tuned_entry
-// chooses among).
-bool has_workspace_free_kernel(int n0, int n1, int n2, int precision, int sign);
 // The autotuner's choice for a geometry at a batch size (memoised per batch
-// bucket like plan creation); nullptr if the geometry has no kernel.
+// bucket like plan creation); nullptr if the geometry has no kernel.  Without
+// `workspace_ok` it chooses among the kernels that need no workspace (a caller
+// that launches on several streams at once and holds none); with it, among all
+// of them, as plan creation does -- the caller then passes a workspace of
+// entry_workspace_bytes to launch_entry.
 const KernelEntry *tuned_entry(int device, int n0, int n1, int n2, int precision, int sign,
-                               long long batch);
+                               long long batch, bool workspace_ok = false);
 
 }  // namespace fft3d

@@ -322,24 +322,16 @@ static const KernelEntry *tune(const std::vector<const KernelEntry *> &cands, in
     return best ? best : cands[0];
 }
 
-bool has_workspace_free_kernel(int n0, int n1, int n2, int precision, int sign)
-{
-    for (const KernelEntry *k : candidates(n0, n1, n2, precision, sign))
-        if (k->family != FAM_TWOPASS) return true;
-    return false;
-}
-
 const KernelEntry *tuned_entry(int device, int n0, int n1, int n2, int precision, int sign,
-                               long long batch)
+                               long long batch, bool workspace_ok)
 {
-    // kernels that need no workspace: the caller launches on several streams at once
     std::vector<const KernelEntry *> cands;
     for (const KernelEntry *k : candidates(n0, n1, n2, precision, sign))
-        if (k->family != FAM_TWOPASS) cands.push_back(k);
+        if (workspace_ok || k->family != FAM_TWOPASS) cands.push_back(k);
     if (cands.empty()) return nullptr;
-    // a memo of its own: plan creation may pick a workspace kernel for the same key
-    static std::map<std::tuple<int, int, int, int, int, int, int>, const KernelEntry *> memo;
-    auto key = std::make_tuple(device, n0, n1, n2, precision, sign, batch_bucket(batch));
+    // a memo of its own, per candidate set
+    static std::map<std::tuple<int, int, int, int, int, int, int, bool>, const KernelEntry *> memo;
+    auto key = std::make_tuple(device, n0, n1, n2, precision, sign, batch_bucket(batch), workspace_ok);
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = memo.find(key);
     if (it != memo.end()) return it->second;

@@ -16,8 +16,8 @@
 // hot loop allocates nothing on the device.
 //
 // A request whose extent is not one of the persistent kernel's kinds (any
-// other compiled extent with a kernel that needs no plan workspace) is
-// launched on its own with its tuned kernel, on the same stream as the batch.
+// other compiled extent) is launched on its own with its tuned kernel, on the
+// same stream as the batch (a scratch-ring kernel with the slot's workspace).
 //
 // Baseline mode (FFT3D_B200_SERVE_PLAIN): every request is launched on its own,
 // as soon as it is admitted, with the tuned per-geometry kernel of its kind --
@@ -72,6 +72,8 @@ struct ServeSlot {
     int *d_err = nullptr;
     BatchItem *h_items = nullptr;  // pinned staging
     BatchSeg *h_segs = nullptr;
+    void *d_work = nullptr;        // workspace of scratch-ring kernels, grown on demand
+    size_t work_bytes = 0;
     bool busy = false;
     std::vector<ServeReq> reqs;
     size_t bytes = 0;
@@ -107,17 +109,50 @@ struct fft3d_b200_server {
     double t_first = 0, t_last = 0;
 };
 
-// Plain mode: the per-geometry kernel the autotuner picks for this request's
-// volume count (memoised by batch size class), and its persistent-grid limit.
+// Plain mode, and extents without a persistent-kernel kind: the per-geometry
+// kernel the autotuner picks for this request's volume count (memoised by batch
+// size class) among the kernels that need no workspace -- they run on many
+// slots at once -- or, for an extent that has none (45^3, 64^3, complex128
+// 30^3), among its scratch-ring kernels; and its persistent-grid limit.
 static const KernelEntry *plain_entry(fft3d_b200_server *s, const ServeReq &r, int *grid)
 {
     const KernelEntry *e = tuned_entry(s->device, r.seg.n0, r.seg.n1, r.seg.n2, r.seg.precision,
                                        r.seg.direction, r.seg.batch);
+    if (!e)
+        e = tuned_entry(s->device, r.seg.n0, r.seg.n1, r.seg.n2, r.seg.precision, r.seg.direction,
+                        r.seg.batch, true);
     if (!e) return nullptr;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
     *grid = entry_occupancy(*e, s->device) * sms;
     return e;
+}
+
+// One request by its own tuned kernel on the slot's stream; a scratch-ring
+// kernel gets the slot's workspace (grown, and its control block zeroed, on
+// first need; every launch leaves the block zero again).  The workspace is
+// allocated and freed in stream order on the slot's stream, so growing it
+// synchronises neither the device nor the other slots.
+static int launch_request(fft3d_b200_server *s, ServeSlot &slot, const ServeReq &r)
+{
+    int grid = 0;
+    const KernelEntry *e = plain_entry(s, r, &grid);
+    if (!e) return FFT3D_B200_ERR_UNSUPPORTED;
+    const size_t wb = entry_workspace_bytes(*e, grid);
+    if (wb > slot.work_bytes) {
+        if (slot.d_work && cudaFreeAsync(slot.d_work, slot.stream) != cudaSuccess) return FFT3D_B200_ERR_CUDA;
+        slot.d_work = nullptr;
+        slot.work_bytes = 0;
+        if (cudaMallocAsync(&slot.d_work, wb, slot.stream) != cudaSuccess) return FFT3D_B200_ERR_NOMEM;
+        if (cudaMemsetAsync(slot.d_work, 0, TWOPASS_CTL_BYTES, slot.stream) != cudaSuccess)
+            return FFT3D_B200_ERR_CUDA;
+        slot.work_bytes = wb;
+    }
+    const double scale = r.seg.direction == FFT3D_B200_BACKWARD ? 1.0 / (double)r.vol_elems : 1.0;
+    if (launch_entry(*e, r.seg.in, r.seg.out, r.seg.batch, scale, slot.stream, grid, slot.d_err,
+                     wb ? slot.d_work : nullptr) != cudaSuccess)
+        return FFT3D_B200_ERR_CUDA;
+    return FFT3D_B200_OK;
 }
 
 // Launch every request of `slot` as one persistent batch (or, in plain mode,
@@ -126,28 +161,14 @@ static int launch_slot(fft3d_b200_server *s, ServeSlot &slot)
 {
     cudaStream_t st = slot.stream;
     if (s->flags & FFT3D_B200_SERVE_PLAIN) {
-        for (const ServeReq &r : slot.reqs) {
-            int grid = 0;
-            const KernelEntry *e = plain_entry(s, r, &grid);
-            if (!e) return FFT3D_B200_ERR_UNSUPPORTED;
-            const double scale = r.seg.direction == FFT3D_B200_BACKWARD ? 1.0 / (double)r.vol_elems : 1.0;
-            if (launch_entry(*e, r.seg.in, r.seg.out, r.seg.batch, scale, st, grid, slot.d_err) !=
-                cudaSuccess)
-                return FFT3D_B200_ERR_CUDA;
-        }
+        for (const ServeReq &r : slot.reqs)
+            if (const int e = launch_request(s, slot, r)) return e;
     } else {
         // requests whose extent is not a kind of the persistent kernel: one
         // tuned launch each on the slot's stream, beside the batch launch
-        for (const ServeReq &r : slot.reqs) {
-            if (r.kind >= 0) continue;
-            int grid = 0;
-            const KernelEntry *e = plain_entry(s, r, &grid);
-            if (!e) return FFT3D_B200_ERR_UNSUPPORTED;
-            const double scale = r.seg.direction == FFT3D_B200_BACKWARD ? 1.0 / (double)r.vol_elems : 1.0;
-            if (launch_entry(*e, r.seg.in, r.seg.out, r.seg.batch, scale, st, grid, slot.d_err) !=
-                cudaSuccess)
-                return FFT3D_B200_ERR_CUDA;
-        }
+        for (const ServeReq &r : slot.reqs)
+            if (r.kind < 0)
+                if (const int e = launch_request(s, slot, r)) return e;
         // descriptors: requests are segments; items largest first
         int nseg = (int)slot.reqs.size();
         std::vector<int> order(nseg);
@@ -316,6 +337,10 @@ static void server_loop(fft3d_b200_server *s)
 static void server_free(fft3d_b200_server *s)
 {
     for (ServeSlot &slot : s->slots) {
+        if (slot.d_work) {  // stream-ordered, before the stream goes
+            cudaFreeAsync(slot.d_work, slot.stream);
+            cudaStreamSynchronize(slot.stream);
+        }
         if (slot.stream) cudaStreamDestroy(slot.stream);
         if (slot.done) cudaEventDestroy(slot.done);
         cudaFree(slot.d_items);
@@ -407,8 +432,7 @@ static int server_submit_at(fft3d_b200_server *s, const fft3d_b200_segment *req,
                            &r.vol_elems, nullptr);
     if (r.kind < 0) {
         // not a kind of the persistent kernel: served by its own tuned launch
-        if (!has_workspace_free_kernel(q.n0, q.n1, q.n2, q.precision, q.direction))
-            return FFT3D_B200_ERR_UNSUPPORTED;
+        if (!fft3d_b200_supports(q.n0, q.n1, q.n2, q.precision)) return FFT3D_B200_ERR_UNSUPPORTED;
         r.vpc = 1;
         r.big = 0;
         r.vol_elems = (long long)q.n0 * q.n1 * q.n2;

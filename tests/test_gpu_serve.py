@@ -152,14 +152,17 @@ def test_admission_budget_and_refusals():
 
 def test_extents_outside_the_batch_kinds():
     """Extents that are not kinds of the persistent batch kernel (9^3, 7x11x13,
-    2x3x5, 32x8x4 here) are served by their own tuned launch in the same slot
-    as the coalesced kinds; every result matches the oracle, and an extent whose
-    only kernels need a plan workspace (45^3) is refused."""
+    2x3x5, 32x8x4, and 45^3 and complex128 30^3, whose kernels need a scratch
+    ring) are served by their own tuned launch in the same slot as the
+    coalesced kinds, a scratch-ring kernel with the slot's workspace; every
+    result matches the oracle, and an extent with no kernel is refused."""
     rng = np.random.default_rng(11)
     specs = [((9, 9, 9), fb.C128, fb.FORWARD, 5), ((7, 11, 13), fb.C64, fb.BACKWARD, 3),
              ((17, 17, 17), fb.C128, fb.FORWARD, 4), ((2, 3, 5), fb.C128, fb.BACKWARD, 7),
              ((8, 8, 8), fb.C64, fb.FORWARD, 30), ((32, 8, 4), fb.C64, fb.FORWARD, 2),
-             ((9, 9, 9), fb.C64, fb.BACKWARD, 2), ((12, 12, 12), fb.C128, fb.BACKWARD, 6)]
+             ((9, 9, 9), fb.C64, fb.BACKWARD, 2), ((12, 12, 12), fb.C128, fb.BACKWARD, 6),
+             ((45, 45, 45), fb.C128, fb.FORWARD, 2), ((30, 30, 30), fb.C128, fb.BACKWARD, 3),
+             ((45, 45, 45), fb.C64, fb.BACKWARD, 2)]
     work = []
     for shape, prec, d, b in specs:
         dt = np.complex128 if prec == fb.C128 else np.complex64
@@ -174,10 +177,10 @@ def test_extents_outside_the_batch_kinds():
     assert srv.stats()["requests"] == len(work)
     lt, lat = srv.latencies()
     assert sorted(int(t) for t in lt) == sorted(tickets)
-    big = torch.zeros(2 * 45 ** 3, dtype=torch.complex128, device="cuda")
+    big = torch.zeros(2 * 14 ** 3, dtype=torch.complex128, device="cuda")
     bo = torch.zeros_like(big)
     with pytest.raises(fb.Fft3dError) as e:
-        srv.submit({"shape": (45, 45, 45), "batch": 2, "in": big.data_ptr(), "out": bo.data_ptr()})
+        srv.submit({"shape": (14, 14, 14), "batch": 2, "in": big.data_ptr(), "out": bo.data_ptr()})
     assert e.value.status == fb.ERR_UNSUPPORTED
     srv.close()
     torch.cuda.synchronize()

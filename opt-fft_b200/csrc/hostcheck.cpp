@@ -9,6 +9,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "staged.cuh"
@@ -40,6 +41,28 @@ static void emulate(const void *vin, void *vout, long long nvol)
         for (int l = 0; l < nv * G::N0 * G::N2; ++l) pass_y<G, S, ALG>(sm.data(), l);
         for (int l = 0; l < nv * G::N1 * G::N2; ++l)
             pass_x_out<G, S, ALG>(sm.data(), l, out + v0 * G::V, scale);
+    }
+}
+
+// The STREAM kernel's bulk-store item (BST): x pass in place, then the stage
+// (natural layout) copied to the output as one block.
+template <int N0, int N1, int N2, typename T, int S, int ALG, int VPC>
+static void emulate_bst(const void *vin, void *vout, long long nvol)
+{
+    using G = Geom<N0, N1, N2, T>;
+    static_assert(G::POL == 0, "bulk stores move natural-layout stages");
+    const cx<T> *in = (const cx<T> *)vin;
+    cx<T> *out = (cx<T> *)vout;
+    std::vector<cx<T>> sm((size_t)VPC * G::PV);
+    const T scale = S > 0 ? T(1) / T(G::V) : T(1);
+    for (long long v0 = 0; v0 < nvol; v0 += VPC) {
+        const int nv = (int)((nvol - v0) < VPC ? (nvol - v0) : VPC);
+        for (auto &e : sm) e = {T(12345.0), T(-6789.0)};
+        for (int g = 0; g < nv * G::V; ++g) stage_in<G>(sm.data(), in + v0 * G::V, g);
+        for (int r = 0; r < nv * G::ROWS; ++r) pass_z<G, S, ALG>(sm.data(), r);
+        for (int l = 0; l < nv * G::N0 * G::N2; ++l) pass_y<G, S, ALG>(sm.data(), l);
+        for (int l = 0; l < nv * G::N1 * G::N2; ++l) pass_x<G, S, ALG>(sm.data(), l, scale);
+        std::copy(sm.begin(), sm.begin() + (size_t)nv * G::V, out + v0 * G::V);
     }
 }
 
@@ -390,6 +413,11 @@ typedef void (*emu_fn)(const void *, void *, long long);
     {L, L, L, sizeof(T) == 8 ? 0 : 1, -1, 200 + PL, 1, &emulate_big_cube<L, T, -1, PL>}, \
     {L, L, L, sizeof(T) == 8 ? 0 : 1, +1, 200 + PL, 1, &emulate_big_cube<L, T, +1, PL>}
 
+#define EMU_BST(N0, N1, N2, T, ALG, VPC)                                                      \
+    {N0, N1, N2, sizeof(T) == 8 ? 0 : 1, -1, 400 + ALG, VPC,                                 \
+     &emulate_bst<N0, N1, N2, T, -1, ALG, VPC>},                                             \
+    {N0, N1, N2, sizeof(T) == 8 ? 0 : 1, +1, 400 + ALG, VPC, &emulate_bst<N0, N1, N2, T, +1, ALG, VPC>}
+
 #define EMU_CL(N0, N1, N2, T, C)                                                             \
     {N0, N1, N2, sizeof(T) == 8 ? 0 : 1, -1, 100 + C, 1,                                   \
      &emulate_cluster<N0, N1, N2, T, -1, C>},                                               \
@@ -458,6 +486,7 @@ static const EmuEntry kEmu[] = {
     EMU(30, 30, 30, float, 0, 1),  EMU(2, 2, 64, float, 0, 24),  EMU(64, 2, 2, float, 0, 16),
     EMU(9, 25, 7, float, 0, 3),    EMU(20, 12, 6, float, 0, 3),  EMU(11, 4, 9, float, 0, 15),
     EMU_TP(30, 30, 30, double, 3), EMU_TP(30, 30, 30, double, 5),
+    EMU_BST(17, 17, 17, double, 0, 1), EMU_BST(17, 17, 17, float, 0, 2),
 };
 
 // The chain kernel's per-CTA loop (chain_kernels.cu k_chain) for one volume per CTA.

@@ -163,6 +163,36 @@ __device__ __forceinline__ void bulk_g2s_hint(void *dst, const void *src, uint32
         : "memory");
 }
 
+// One-dimensional bulk copy shared -> global (TMA, no tensor map) in this
+// thread's current bulk group.  dst, src 16-byte aligned; bytes % 16 == 0.
+__device__ __forceinline__ void bulk_s2g(void *dst, const void *src, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
+                 "r"(smem_u32(src)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit()
+{
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+
+// Wait until at most N of this thread's bulk groups still read their shared-memory
+// source (the source may then be overwritten).
+template <int N>
+__device__ __forceinline__ void bulk_wait_read()
+{
+    asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+
+// Wait until at most N of this thread's bulk groups are incomplete (their
+// writes performed).
+template <int N>
+__device__ __forceinline__ void bulk_wait()
+{
+    asm volatile("cp.async.bulk.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // L2-only stores of one complex value with an L2 cache policy.
 __device__ __forceinline__ void st_cg_hint(double2 *p, double2 v, uint64_t policy)
 {

@@ -7,7 +7,10 @@
 // so HBM reads overlap the arithmetic; the x pass writes results straight to HBM
 // with coalesced streaming stores, so a stage is free again as soon as its last
 // pass has read it.  NSTAGE = 1 with MINB = 2 puts two single-stage CTAs on an
-// SM instead: one loads while the other computes.
+// SM instead: one loads while the other computes.  BST variants ("bst") run the
+// x pass in place and move the finished group to HBM with one bulk copy (TMA)
+// issued by thread 0, so no thread waits on its output stores; the stage is
+// refilled after the next item's z pass, once that copy has read it.
 //
 // Loaders:
 //   BULK   (natural layout, odd n2): thread 0 issues one cp.async.bulk (TMA)
@@ -67,12 +70,14 @@ __device__ __forceinline__ void cp_async_wait_pending(int pending)
     }
 }
 
-template <class G, int S, int ALG, int VPC, int NT, int LOADER, int NSTAGE, int MINB>
+template <class G, int S, int ALG, int VPC, int NT, int LOADER, int NSTAGE, int MINB, bool BST>
 __global__ void __launch_bounds__(NT, MINB)
     k_stream(const cx<typename G::T> *__restrict__ in, cx<typename G::T> *__restrict__ out,
              long long nvol, typename G::T scale, int *err)
 {
     static_assert(NSTAGE >= 1 && NSTAGE <= 4, "ring depth");
+    static_assert(!BST || (LOADER == LOADER_BULK && NSTAGE >= 2),
+                  "bulk stores move natural-layout stages of a ring at least two deep");
     pdl_begin();
     using T = typename G::T;
     using SL = StreamLayout<G, VPC, NSTAGE>;
@@ -131,7 +136,8 @@ __global__ void __launch_bounds__(NT, MINB)
     for (; item < nitems; item += stride, ++k) {
         const int cur = k % NSTAGE;
         const long long ahead = item + (long long)(NSTAGE - 1) * stride;
-        if (ahead < nitems) issue(ahead, (k + NSTAGE - 1) % NSTAGE);
+        if constexpr (!BST)
+            if (ahead < nitems) issue(ahead, (k + NSTAGE - 1) % NSTAGE);
 
         if constexpr (LOADER == LOADER_BULK) {
             if (!mbar_wait_bounded(&bar[cur], (uint32_t)((k / NSTAGE) & 1))) s_abort = 1;
@@ -148,31 +154,56 @@ __global__ void __launch_bounds__(NT, MINB)
         const int nv = (int)((nvol - v0) < VPC ? (nvol - v0) : VPC);
         cx<T> *sm = stage(cur);
         for (int r = tid; r < nv * G::ROWS; r += NT) pass_z<G, S, ALG>(sm, r);
+        if constexpr (BST)  // the stage refilled next held the previous item: its store has read it
+            if (tid == 0) bulk_wait_read<0>();
         __syncthreads();
+        if constexpr (BST)
+            if (ahead < nitems) issue(ahead, (k + NSTAGE - 1) % NSTAGE);
         for (int l = tid; l < nv * G::N0 * G::N2; l += NT) pass_y<G, S, ALG>(sm, l);
         __syncthreads();
         cx<T> *gout = out + v0 * G::V;
-        // plain stores: a following transform of this output finds its last part in L2
-        for (int l = tid; l < nv * G::N1 * G::N2; l += NT) pass_x_out<G, S, ALG, true>(sm, l, gout, scale);
-        if constexpr (LOADER == LOADER_BULK) fence_proxy_async_smem();
-        __syncthreads();
+        if constexpr (BST) {
+            // x pass in place, then one bulk store of the group (plain L2 policy:
+            // a following transform of this output finds its last part in L2)
+            for (int l = tid; l < nv * G::N1 * G::N2; l += NT) pass_x<G, S, ALG>(sm, l, scale);
+            fence_proxy_async_smem();
+            __syncthreads();
+            const uint32_t bytes = (uint32_t)(nv * G::V) * (uint32_t)G::EB;
+            if (((((uintptr_t)gout) | bytes) & 15u) == 0) {
+                if (tid == 0) {
+                    bulk_s2g(gout, sm, bytes);
+                    bulk_commit();
+                }
+            } else {
+                for (int g = tid; g < nv * G::V; g += NT) gout[g] = sm[g];
+                fence_proxy_async_smem();
+            }
+        } else {
+            // plain stores: a following transform of this output finds its last part in L2
+            for (int l = tid; l < nv * G::N1 * G::N2; l += NT) pass_x_out<G, S, ALG, true>(sm, l, gout, scale);
+            if constexpr (LOADER == LOADER_BULK) fence_proxy_async_smem();
+            __syncthreads();
+        }
     }
 
     if (s_abort) {
         if (tid == 0) report_error(err, DEV_ERR_LOAD_TIMEOUT);
         // bounded drain of the stage that timed out and of the loads issued ahead of it
         if constexpr (LOADER == LOADER_BULK) {
-            for (int j = 0; j < NSTAGE; ++j)
+            // BST issues an item's look-ahead load after its wait: one fewer in flight
+            for (int j = 0; j < NSTAGE - (BST ? 1 : 0); ++j)
                 if (item + j * stride < nitems)
                     mbar_wait_bounded(&bar[(k + j) % NSTAGE], (uint32_t)(((k + j) / NSTAGE) & 1));
         } else {
             cp_async_wait<0>();
         }
     }
+    if constexpr (BST)  // the stores read this CTA's shared memory until they complete
+        if (tid == 0) bulk_wait<0>();
 }
 
 template <int N0, int N1, int N2, typename T, int S, int ALG, int VPC, int NT, int NSTAGE,
-          int MINB>
+          int MINB, bool BST = false>
 static void add_stream(std::vector<KernelEntry> &out, const char *name)
 {
     using G = Geom<N0, N1, N2, T>;
@@ -188,7 +219,7 @@ static void add_stream(std::vector<KernelEntry> &out, const char *name)
     e.vpc = VPC;
     e.threads = NT;
     e.smem = StreamLayout<G, VPC, NSTAGE>::SMEM_BYTES;
-    e.func = (const void *)&k_stream<G, S, ALG, VPC, NT, LOADER, NSTAGE, MINB>;
+    e.func = (const void *)&k_stream<G, S, ALG, VPC, NT, LOADER, NSTAGE, MINB, BST>;
     e.name = name;
     out.push_back(e);
 }
@@ -200,6 +231,15 @@ static void add_stream(std::vector<KernelEntry> &out, const char *name)
     add_stream<N0, N1, N2, T, +1, ALG, VPC, NT, NST, MINB>(                                       \
         out, "stream " #N0 "x" #N1 "x" #N2 " " #T " alg" #ALG " vpc" #VPC " nt" #NT " st" #NST   \
              " minb" #MINB)
+
+// The x pass in place and one bulk store per item (natural layouts, odd n2).
+#define FFT3D_STREAM_BST(N0, N1, N2, T, ALG, VPC, NT, NST, MINB)                                  \
+    add_stream<N0, N1, N2, T, -1, ALG, VPC, NT, NST, MINB, true>(                                 \
+        out, "stream " #N0 "x" #N1 "x" #N2 " " #T " alg" #ALG " vpc" #VPC " nt" #NT " st" #NST   \
+             " minb" #MINB " bst");                                                               \
+    add_stream<N0, N1, N2, T, +1, ALG, VPC, NT, NST, MINB, true>(                                 \
+        out, "stream " #N0 "x" #N1 "x" #N2 " " #T " alg" #ALG " vpc" #VPC " nt" #NT " st" #NST   \
+             " minb" #MINB " bst")
 
 void register_stream_kernels(std::vector<KernelEntry> &out)
 {
@@ -218,6 +258,7 @@ void register_stream_kernels(std::vector<KernelEntry> &out)
     FFT3D_STREAM(17, 17, 17, double, 0, 1, 320, 2, 1);
     FFT3D_STREAM(17, 17, 17, double, 1, 1, 320, 2, 1);
     FFT3D_STREAM(17, 17, 17, double, 0, 1, 320, 1, 2);
+    FFT3D_STREAM_BST(17, 17, 17, double, 0, 1, 320, 2, 1);
     FFT3D_STREAM(8, 8, 16, double, 0, 4, 512, 2, 1);
     FFT3D_STREAM(8, 8, 16, double, 0, 2, 256, 4, 1);
     FFT3D_STREAM(13, 13, 13, double, 0, 1, 192, 3, 2);
@@ -233,6 +274,7 @@ void register_stream_kernels(std::vector<KernelEntry> &out)
     FFT3D_STREAM(16, 16, 16, float, 0, 2, 512, 2, 1);
     FFT3D_STREAM(17, 17, 17, float, 0, 2, 640, 2, 1);
     FFT3D_STREAM(17, 17, 17, float, 1, 2, 640, 2, 1);
+    FFT3D_STREAM_BST(17, 17, 17, float, 0, 2, 640, 2, 1);
     FFT3D_STREAM(8, 8, 16, float, 0, 4, 512, 4, 1);
     FFT3D_STREAM(8, 8, 16, float, 0, 8, 512, 2, 1);
     FFT3D_STREAM(16, 16, 32, float, 0, 1, 256, 2, 1);

@@ -184,6 +184,30 @@ FFT_HD void pass_x_out(const cx<typename G::T> *sm, int l, cx<typename G::T> *go
     }
 }
 
+// Pass along x for line l = (vol*N1 + y)*N2 + z in place in shared memory,
+// scaled for the inverse: for kernels that move the finished stage to HBM with
+// one bulk copy instead of storing from registers.
+template <class G, int S, int ALG>
+FFT_HD void pass_x(cx<typename G::T> *sm, int l, typename G::T scale)
+{
+    static_assert(!x_direct_sum(G::N0), "long prime x lines are summed out of shared memory");
+    using T = typename G::T;
+    const int z = l % G::N2;
+    const int t = l / G::N2;
+    const int y = t % G::N1;
+    const int vol = t / G::N1;
+    cx<T> v[G::N0];
+#pragma unroll
+    for (int j = 0; j < G::N0; ++j) v[j] = sm[G::off((vol * G::N0 + j) * G::N1 + y, z)];
+    dft<G::N0, S, T, ALG>(v);
+#pragma unroll
+    for (int j = 0; j < G::N0; ++j) {
+        cx<T> r = v[j];
+        if constexpr (S > 0) r = cscale(r, scale);
+        sm[G::off((vol * G::N0 + j) * G::N1 + y, z)] = r;
+    }
+}
+
 // Chain-step epilogues applied to each output point of the last pass.
 constexpr int EPI_UNITARY = 1;  // state <- FFT(state) * V^(-1/2)
 constexpr int EPI_MAP = 2;      // z = FFT(state) + c;  state <- z / (1 + |z|)

@@ -105,6 +105,22 @@ def test_cluster_data_movement(hostcheck, prec, c, sign):
     assert err < (C128_TOL if prec == 0 else C64_TOL), err
 
 
+@pytest.mark.parametrize("prec,vpc,nvol", [(0, 1, 3), (1, 2, 3)])
+@pytest.mark.parametrize("sign", [-1, +1])
+def test_stream_bulk_store_item(hostcheck, prec, vpc, nvol, sign):
+    """The STREAM kernel's bulk-store item (alg = 400 + ALG): x pass in place and
+    the natural-layout stage copied out whole, a partial group included."""
+    shape = (17, 17, 17)
+    rng = np.random.default_rng(3500 + prec)
+    dt = np.complex128 if prec == 0 else np.complex64
+    x = field(rng, (nvol,) + shape, dtype=dt)
+    got = run(hostcheck, x, shape, prec, sign, 400, vpc)
+    x64 = x.astype(np.complex128)
+    want = oracle.fft3d(x64) if sign < 0 else oracle.ifft3d(x64)
+    err = oracle.rel_error_per_volume(got, want).max()
+    assert err < (C128_TOL if prec == 0 else C64_TOL), err
+
+
 @pytest.mark.parametrize("n,prec,pl", [(36, 0, 4), (36, 1, 6), (36, 1, 4)])
 @pytest.mark.parametrize("sign", [-1, +1])
 def test_two_phase_cube(hostcheck, n, prec, pl, sign):

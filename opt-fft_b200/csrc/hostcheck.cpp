@@ -487,6 +487,8 @@ static const EmuEntry kEmu[] = {
     EMU(9, 25, 7, float, 0, 3),    EMU(20, 12, 6, float, 0, 3),  EMU(11, 4, 9, float, 0, 15),
     EMU_TP(30, 30, 30, double, 3), EMU_TP(30, 30, 30, double, 5),
     EMU_BST(17, 17, 17, double, 0, 1), EMU_BST(17, 17, 17, float, 0, 2),
+    EMU_BST(13, 13, 13, double, 0, 1), EMU_BST(13, 13, 13, double, 0, 2),
+    EMU_BST(13, 13, 13, float, 0, 2),
 };
 
 // The chain kernel's per-CTA loop (chain_kernels.cu k_chain) for one volume per CTA.

@@ -263,6 +263,8 @@ void register_stream_kernels(std::vector<KernelEntry> &out)
     FFT3D_STREAM(8, 8, 16, double, 0, 2, 256, 4, 1);
     FFT3D_STREAM(13, 13, 13, double, 0, 1, 192, 3, 2);
     FFT3D_STREAM(13, 13, 13, double, 0, 2, 352, 2, 1);
+    FFT3D_STREAM_BST(13, 13, 13, double, 0, 1, 192, 3, 2);
+    FFT3D_STREAM_BST(13, 13, 13, double, 0, 2, 352, 2, 1);
     // complex float
     FFT3D_STREAM(6, 6, 6, float, 0, 16, 576, 3, 1);
     FFT3D_STREAM(6, 6, 6, float, 0, 32, 1024, 2, 1);
@@ -280,6 +282,7 @@ void register_stream_kernels(std::vector<KernelEntry> &out)
     FFT3D_STREAM(16, 16, 32, float, 0, 1, 256, 2, 1);
     FFT3D_STREAM(16, 16, 32, float, 0, 1, 256, 3, 1);
     FFT3D_STREAM(13, 13, 13, float, 0, 2, 352, 3, 1);
+    FFT3D_STREAM_BST(13, 13, 13, float, 0, 2, 352, 3, 1);
     FFT3D_STREAM(23, 23, 23, float, 0, 1, 288, 2, 1);
 }
 

@@ -105,13 +105,17 @@ def test_cluster_data_movement(hostcheck, prec, c, sign):
     assert err < (C128_TOL if prec == 0 else C64_TOL), err
 
 
-@pytest.mark.parametrize("prec,vpc,nvol", [(0, 1, 3), (1, 2, 3)])
+BST = [((17, 17, 17), 0, 1, 3), ((17, 17, 17), 1, 2, 3), ((13, 13, 13), 0, 1, 2),
+       ((13, 13, 13), 0, 2, 3), ((13, 13, 13), 1, 2, 3)]
+
+
+@pytest.mark.parametrize("shape,prec,vpc,nvol", BST,
+                         ids=[f"{t[0]}-c{128 if t[1] == 0 else 64}-vpc{t[2]}" for t in BST])
 @pytest.mark.parametrize("sign", [-1, +1])
-def test_stream_bulk_store_item(hostcheck, prec, vpc, nvol, sign):
+def test_stream_bulk_store_item(hostcheck, shape, prec, vpc, nvol, sign):
     """The STREAM kernel's bulk-store item (alg = 400 + ALG): x pass in place and
     the natural-layout stage copied out whole, a partial group included."""
-    shape = (17, 17, 17)
-    rng = np.random.default_rng(3500 + prec)
+    rng = np.random.default_rng(3500 + prec + shape[0])
     dt = np.complex128 if prec == 0 else np.complex64
     x = field(rng, (nvol,) + shape, dtype=dt)
     got = run(hostcheck, x, shape, prec, sign, 400, vpc)

@@ -44,13 +44,17 @@ static void emulate(const void *vin, void *vout, long long nvol)
     }
 }
 
-// The STREAM kernel's bulk-store item (BST): x pass in place, then the stage
-// (natural layout) copied to the output as one block.
+// The STREAM kernel's bulk-store item (BST): the x pass leaves the stage in
+// natural layout (in place for natural layouts; padded and swizzled ones read
+// every line into registers before any line is stored at its natural place),
+// then the stage is copied to the output as one block.
 template <int N0, int N1, int N2, typename T, int S, int ALG, int VPC>
 static void emulate_bst(const void *vin, void *vout, long long nvol)
 {
     using G = Geom<N0, N1, N2, T>;
-    static_assert(G::POL == 0, "bulk stores move natural-layout stages");
+    struct Line {
+        cx<T> v[N0];
+    };
     const cx<T> *in = (const cx<T> *)vin;
     cx<T> *out = (cx<T> *)vout;
     std::vector<cx<T>> sm((size_t)VPC * G::PV);
@@ -61,7 +65,14 @@ static void emulate_bst(const void *vin, void *vout, long long nvol)
         for (int g = 0; g < nv * G::V; ++g) stage_in<G>(sm.data(), in + v0 * G::V, g);
         for (int r = 0; r < nv * G::ROWS; ++r) pass_z<G, S, ALG>(sm.data(), r);
         for (int l = 0; l < nv * G::N0 * G::N2; ++l) pass_y<G, S, ALG>(sm.data(), l);
-        for (int l = 0; l < nv * G::N1 * G::N2; ++l) pass_x<G, S, ALG>(sm.data(), l, scale);
+        if constexpr (G::POL == 0) {
+            for (int l = 0; l < nv * G::N1 * G::N2; ++l) pass_x<G, S, ALG>(sm.data(), l, scale);
+        } else {
+            std::vector<Line> regs((size_t)nv * G::N1 * G::N2);
+            for (int l = 0; l < nv * G::N1 * G::N2; ++l)
+                pass_x_regs<G, S, ALG>(sm.data(), l, scale, regs[l].v);
+            for (int l = 0; l < nv * G::N1 * G::N2; ++l) store_x_natural<G>(sm.data(), l, regs[l].v);
+        }
         std::copy(sm.begin(), sm.begin() + (size_t)nv * G::V, out + v0 * G::V);
     }
 }
@@ -488,7 +499,8 @@ static const EmuEntry kEmu[] = {
     EMU_TP(30, 30, 30, double, 3), EMU_TP(30, 30, 30, double, 5),
     EMU_BST(17, 17, 17, double, 0, 1), EMU_BST(17, 17, 17, float, 0, 2),
     EMU_BST(13, 13, 13, double, 0, 1), EMU_BST(13, 13, 13, double, 0, 2),
-    EMU_BST(13, 13, 13, float, 0, 2),
+    EMU_BST(13, 13, 13, float, 0, 2),  EMU_BST(8, 8, 8, double, 0, 1),
+    EMU_BST(16, 16, 16, double, 0, 1), EMU_BST(16, 16, 16, float, 0, 1),
 };
 
 // The chain kernel's per-CTA loop (chain_kernels.cu k_chain) for one volume per CTA.

@@ -7,10 +7,13 @@
 // so HBM reads overlap the arithmetic; the x pass writes results straight to HBM
 // with coalesced streaming stores, so a stage is free again as soon as its last
 // pass has read it.  NSTAGE = 1 with MINB = 2 puts two single-stage CTAs on an
-// SM instead: one loads while the other computes.  BST variants ("bst") run the
-// x pass in place and move the finished group to HBM with one bulk copy (TMA)
-// issued by thread 0, so no thread waits on its output stores; the stage is
-// refilled after the next item's z pass, once that copy has read it.
+// SM instead: one loads while the other computes.  BST variants ("bst") leave
+// the x pass's results in the stage in natural layout and move the finished
+// group to HBM with one bulk copy (TMA) issued by thread 0, so no thread waits on
+// its output stores; the stage is refilled after the next item's z pass, once
+// that copy has read it.  Natural layouts transform the x lines in place; padded
+// and swizzled ones (one x line per thread) transform into registers and, after
+// a barrier, store the lines at their natural places.
 //
 // Loaders:
 //   BULK   (natural layout, odd n2): thread 0 issues one cp.async.bulk (TMA)
@@ -76,8 +79,9 @@ __global__ void __launch_bounds__(NT, MINB)
              long long nvol, typename G::T scale, int *err)
 {
     static_assert(NSTAGE >= 1 && NSTAGE <= 4, "ring depth");
-    static_assert(!BST || (LOADER == LOADER_BULK && NSTAGE >= 2),
-                  "bulk stores move natural-layout stages of a ring at least two deep");
+    static_assert(!BST || NSTAGE >= 2, "bulk stores need a ring at least two deep");
+    static_assert(!BST || G::POL == 0 || VPC * G::N1 * G::N2 <= NT,
+                  "padded or swizzled layouts re-lay one x line per thread");
     pdl_begin();
     using T = typename G::T;
     using SL = StreamLayout<G, VPC, NSTAGE>;
@@ -142,8 +146,8 @@ __global__ void __launch_bounds__(NT, MINB)
         if constexpr (LOADER == LOADER_BULK) {
             if (!mbar_wait_bounded(&bar[cur], (uint32_t)((k / NSTAGE) & 1))) s_abort = 1;
         } else {
-            int later = 0;  // groups committed after this item's
-            for (int j = 1; j < NSTAGE; ++j)
+            int later = 0;  // groups committed after this item's (BST issues its look-ahead later)
+            for (int j = 1; j < NSTAGE - (BST ? 1 : 0); ++j)
                 if (item + j * stride < nitems) ++later;
             cp_async_wait_pending(later);
         }
@@ -165,7 +169,15 @@ __global__ void __launch_bounds__(NT, MINB)
         if constexpr (BST) {
             // x pass in place, then one bulk store of the group (plain L2 policy:
             // a following transform of this output finds its last part in L2)
-            for (int l = tid; l < nv * G::N1 * G::N2; l += NT) pass_x<G, S, ALG>(sm, l, scale);
+            if constexpr (G::POL == 0) {
+                for (int l = tid; l < nv * G::N1 * G::N2; l += NT) pass_x<G, S, ALG>(sm, l, scale);
+            } else {
+                cx<T> v[G::N0];
+                const bool line = tid < nv * G::N1 * G::N2;
+                if (line) pass_x_regs<G, S, ALG>(sm, tid, scale, v);
+                __syncthreads();
+                if (line) store_x_natural<G>(sm, tid, v);
+            }
             fence_proxy_async_smem();
             __syncthreads();
             const uint32_t bytes = (uint32_t)(nv * G::V) * (uint32_t)G::EB;
@@ -190,7 +202,7 @@ __global__ void __launch_bounds__(NT, MINB)
         if (tid == 0) report_error(err, DEV_ERR_LOAD_TIMEOUT);
         // bounded drain of the stage that timed out and of the loads issued ahead of it
         if constexpr (LOADER == LOADER_BULK) {
-            // BST issues an item's look-ahead load after its wait: one fewer in flight
+            // BST issues an item's look-ahead load after its z pass: one fewer in flight
             for (int j = 0; j < NSTAGE - (BST ? 1 : 0); ++j)
                 if (item + j * stride < nitems)
                     mbar_wait_bounded(&bar[(k + j) % NSTAGE], (uint32_t)(((k + j) / NSTAGE) & 1));
@@ -251,10 +263,12 @@ void register_stream_kernels(std::vector<KernelEntry> &out)
     FFT3D_STREAM(8, 8, 8, double, 0, 8, 512, 2, 1);
     FFT3D_STREAM(8, 8, 8, double, 0, 1, 64, 3, 8);   // one volume per item: even tails
     FFT3D_STREAM(8, 8, 8, double, 0, 1, 64, 4, 6);
+    FFT3D_STREAM_BST(8, 8, 8, double, 0, 1, 64, 4, 6);
     FFT3D_STREAM(12, 12, 12, double, 0, 2, 288, 2, 1);
     FFT3D_STREAM(12, 12, 12, double, 0, 1, 160, 3, 2);
     FFT3D_STREAM(16, 16, 16, double, 0, 1, 256, 2, 1);
     FFT3D_STREAM(16, 16, 16, double, 0, 1, 256, 3, 1);
+    FFT3D_STREAM_BST(16, 16, 16, double, 0, 1, 256, 3, 1);
     FFT3D_STREAM(17, 17, 17, double, 0, 1, 320, 2, 1);
     FFT3D_STREAM(17, 17, 17, double, 1, 1, 320, 2, 1);
     FFT3D_STREAM(17, 17, 17, double, 0, 1, 320, 1, 2);
@@ -273,6 +287,7 @@ void register_stream_kernels(std::vector<KernelEntry> &out)
     FFT3D_STREAM(12, 12, 12, float, 0, 2, 288, 4, 1);
     FFT3D_STREAM(12, 12, 12, float, 0, 4, 576, 2, 1);
     FFT3D_STREAM(16, 16, 16, float, 0, 1, 256, 4, 1);
+    FFT3D_STREAM_BST(16, 16, 16, float, 0, 1, 256, 4, 1);
     FFT3D_STREAM(16, 16, 16, float, 0, 2, 512, 2, 1);
     FFT3D_STREAM(17, 17, 17, float, 0, 2, 640, 2, 1);
     FFT3D_STREAM(17, 17, 17, float, 1, 2, 640, 2, 1);

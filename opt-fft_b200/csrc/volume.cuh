@@ -208,6 +208,39 @@ FFT_HD void pass_x(cx<typename G::T> *sm, int l, typename G::T scale)
     }
 }
 
+// Pass along x for line l into registers (scaled for the inverse), and the
+// matching store of the line at its natural (unpadded, unswizzled) place in the
+// same buffer.  Kernels with padded or swizzled layouts and one x line per
+// thread run the first for every line, wait at a barrier (a natural slot may
+// hold a point another thread has not read yet), then the second, and move the
+// natural-layout stage to HBM with one bulk copy.
+template <class G, int S, int ALG>
+FFT_HD void pass_x_regs(const cx<typename G::T> *sm, int l, typename G::T scale,
+                        cx<typename G::T> (&v)[G::N0])
+{
+    static_assert(!x_direct_sum(G::N0), "long prime x lines are summed out of shared memory");
+    const int z = l % G::N2;
+    const int t = l / G::N2;
+    const int y = t % G::N1;
+    const int vol = t / G::N1;
+#pragma unroll
+    for (int j = 0; j < G::N0; ++j) v[j] = sm[G::off((vol * G::N0 + j) * G::N1 + y, z)];
+    dft<G::N0, S, typename G::T, ALG>(v);
+    if constexpr (S > 0) {
+#pragma unroll
+        for (int j = 0; j < G::N0; ++j) v[j] = cscale(v[j], scale);
+    }
+}
+
+template <class G>
+FFT_HD void store_x_natural(cx<typename G::T> *sm, int l, const cx<typename G::T> (&v)[G::N0])
+{
+    const int zy = l % (G::N1 * G::N2);  // y*N2 + z
+    const int vol = l / (G::N1 * G::N2);
+#pragma unroll
+    for (int j = 0; j < G::N0; ++j) sm[vol * G::V + j * (G::N1 * G::N2) + zy] = v[j];
+}
+
 // Chain-step epilogues applied to each output point of the last pass.
 constexpr int EPI_UNITARY = 1;  // state <- FFT(state) * V^(-1/2)
 constexpr int EPI_MAP = 2;      // z = FFT(state) + c;  state <- z / (1 + |z|)

@@ -106,7 +106,9 @@ def test_cluster_data_movement(hostcheck, prec, c, sign):
 
 
 BST = [((17, 17, 17), 0, 1, 3), ((17, 17, 17), 1, 2, 3), ((13, 13, 13), 0, 1, 2),
-       ((13, 13, 13), 0, 2, 3), ((13, 13, 13), 1, 2, 3)]
+       ((13, 13, 13), 0, 2, 3), ((13, 13, 13), 1, 2, 3),
+       # swizzled layouts: x lines re-laid through registers
+       ((8, 8, 8), 0, 1, 3), ((16, 16, 16), 0, 1, 2), ((16, 16, 16), 1, 1, 2)]
 
 
 @pytest.mark.parametrize("shape,prec,vpc,nvol", BST,

@@ -899,16 +899,30 @@ static int run_host_chain(fft3d_b200_plan *const *plans, int nplans, const void 
         // their own, each chunk's steps ordered by events, so no upload waits
         // for an earlier download
         cudaStream_t up = p->xs[0], down = p->xs[1], comp = p->stream;
+        // Copy boundaries on 64 KB: DMA from or to offsets that are only
+        // 16-byte aligned runs markedly slower.  Upload c ends at the boundary
+        // at or after chunk c's last volume (it may carry the head of chunk
+        // c+1), download c at the boundary at or before it (only finished
+        // results), so each chunk still waits for one upload and one transform.
+        const size_t total = off[nchunks];
+        const size_t A = (size_t)64 << 10;
+        auto up_end = [&](size_t c) { return c + 1 == nchunks ? total : std::min(total, (off[c + 1] + A - 1) / A * A); };
+        auto down_end = [&](size_t c) { return c + 1 == nchunks ? total : off[c + 1] / A * A; };
+        const char *res_base = (nplans & 1) ? (const char *)p->d_out : (const char *)p->d_in;
+        size_t ua = 0, da = 0;
         for (size_t c = 0; c < nchunks; ++c) {
             char *din = (char *)p->d_in + off[c];
             char *dout = (char *)p->d_out + off[c];
             char *res = nullptr;
-            if (cudaMemcpyAsync(din, src + off[c], chunk_len(c), cudaMemcpyHostToDevice, up) != cudaSuccess ||
+            const size_t ub = std::max(ua, up_end(c)), db = std::max(da, down_end(c));
+            if ((ub > ua && cudaMemcpyAsync((char *)p->d_in + ua, src + ua, ub - ua, cudaMemcpyHostToDevice, up) != cudaSuccess) ||
                 cudaEventRecord(p->ev[0], up) != cudaSuccess || cudaStreamWaitEvent(comp, p->ev[0], 0) != cudaSuccess ||
                 !transform(din, dout, sizes[c], comp, 0, &res) || cudaEventRecord(p->ev[1], comp) != cudaSuccess ||
                 cudaStreamWaitEvent(down, p->ev[1], 0) != cudaSuccess ||
-                cudaMemcpyAsync(dst + off[c], res, chunk_len(c), cudaMemcpyDeviceToHost, down) != cudaSuccess)
+                (db > da && cudaMemcpyAsync(dst + da, res_base + da, db - da, cudaMemcpyDeviceToHost, down) != cudaSuccess))
                 return FFT3D_B200_ERR_CUDA;
+            ua = ub;
+            da = db;
         }
         if (cudaStreamSynchronize(down) != cudaSuccess || cudaStreamSynchronize(comp) != cudaSuccess ||
             cudaStreamSynchronize(up) != cudaSuccess)

@@ -212,6 +212,32 @@ def test_pinned_host_chain_with_scratch_kernels():
     assert np.array_equal(pin_in.numpy(), x)
 
 
+@pytest.mark.parametrize("shape,prec,B", [((17, 17, 17), fb.C128, 61), ((13, 13, 13), fb.C64, 301)])
+def test_pinned_host_chain_unaligned_chunks(monkeypatch, shape, prec, B):
+    """Page-locked buffers cut into 1 MB chunks of whole volumes whose
+    boundaries are not 64 KB multiples: the copies run between 64 KB
+    boundaries (an upload may carry the head of the next chunk, a download
+    stops short of the current chunk's end), so every byte still arrives
+    once and after its transform.  One, two and three plans (the result
+    alternates between the two device buffers) give the device path's bits."""
+    monkeypatch.setenv("FFT3D_B200_HOST_CHUNK_MB", "1")  # read when a plan first stages
+    rng = np.random.default_rng(B)
+    x = field(rng, (B,) + shape, dtype=NDT[prec])
+    f = fb.Plan(shape, B, fb.FORWARD, prec)
+    i = fb.Plan(shape, B, fb.BACKWARD, prec)
+    pin_in = torch.from_numpy(x).pin_memory()
+    pin_out = torch.empty_like(pin_in).pin_memory()
+    arr = (ctypes.c_void_p * 3)(f.handle.value, i.handle.value, f.handle.value)
+    fwd, _ = run_plan(f, x)
+    back, _ = run_plan(i, fwd)
+    fwd2, _ = run_plan(f, back)
+    for n, want in ((1, fwd), (2, back), (3, fwd2)):
+        pin_out.zero_()
+        assert fb.lib().fft3d_b200_execute_host_chain(arr, n, pin_in.data_ptr(), pin_out.data_ptr()) == 0
+        assert np.array_equal(pin_out.numpy(), want), n
+    assert np.array_equal(pin_in.numpy(), x)
+
+
 # ---------------------------------------------------------------- edges and errors
 
 def test_edges_and_errors():

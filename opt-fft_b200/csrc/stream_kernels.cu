@@ -104,10 +104,12 @@ __global__ void __launch_bounds__(NT, MINB)
 
     // Issue the load of `item` into stage s.  For BULK, returns with the copy in
     // flight (or, for an unaligned item, done by the threads and arrived).
-    // Inverse transforms walk their items from the last to the first: after a
-    // forward transform (which walks them in order) the volumes it wrote last
-    // are still in L2 when the inverse starts, and are read first.
-    auto phys = [&](long long item) { return S > 0 ? nitems - 1 - item : item; };
+    // Both directions walk their items in order.  Starting an inverse on the
+    // items a preceding forward wrote last (still partly in L2) -- walking them
+    // from last to first, or from the last 32 MB of the batch and wrapping --
+    // measured 0.6% slower over a forward + inverse step and 4-5% slower for an
+    // inverse alone.
+    auto phys = [&](long long item) { return item; };
     const uint64_t pol_first = l2_policy_evict_first();
     auto issue = [&](long long item, int s) {
         const long long v0 = phys(item) * VPC;

@@ -84,13 +84,15 @@ def test_every_variant_matches_oracle(shape, prec, direction):
         tol = 3e-5 if "split2" in v else (C128_TOL if prec == fb.C128 else C64_TOL)
         b = batch_for(shape, prec)
         if v.startswith("stream"):
-            # persistent kernels: every CTA walks >= 2 groups and one group is partial
+            # persistent kernels: every CTA walks >= 2 groups and, for groups of
+            # several volumes, the last group is partial (for complex64 17^3 and
+            # 13^3 a group that is not 16-byte aligned: the threads' copy paths)
             vpc = int(v.split(" vpc")[1].split()[0])
-            b = 2 * 148 * vpc + vpc // 2 + 1
+            b = 2 * 148 * vpc + (vpc + 1) // 2
         elif v.startswith("volume"):
             # several CTAs and a partial group
             vpc = int(v.split(" vpc")[1].split()[0])
-            b = max(b, 2 * vpc + vpc // 2 + 1)
+            b = max(b, 2 * vpc + (vpc + 1) // 2)
         elif v.startswith("twopass"):
             # beyond the scratch ring (about 40 volumes at a full grid): slots are reused
             b = 100

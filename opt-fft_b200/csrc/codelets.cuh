@@ -10,6 +10,8 @@
 //   N = 3                     Winograd 3-point
 //   N odd prime (or odd with no better split)
 //                             conjugate-pair folded direct sum: (N-1)^2 real FMA
+//   N = 17, ALG_CRT           the folded sum with its cosine half as a length-8
+//                             cyclic convolution through a CRT split (dft17_crt)
 //   N = 17, ALG_RADER         Rader (python/fft3d.py:204-245): the 16 non-zero
 //                             inputs permuted by the primitive root 3 and a
 //                             length-16 cyclic convolution through a 16-point FFT,
@@ -101,6 +103,9 @@ constexpr int tw_off(int n) { return n * (n - 1) / 2; }   // N = 1..TW_MAXN, pac
 constexpr int TW_ENTRIES = tw_off(TW_MAXN + 1);            // 2080
 // Rader-17 kernel spectra: [sign index][16], sign index 0 = forward, 1 = backward.
 constexpr int RADER17_ENTRIES = 32;
+// CRT-17 kernel residues (dft17_crt): the cosine kernel c[m] = cos(2*pi*3^m/17),
+// m = 0..7, reduced mod x-1, x+1 (scaled 1/8), x^2+1 (1/4) and x^4+1 (1/2).
+constexpr int CRT17_ENTRIES = 8;
 // Line lengths above TW_MAXN: one table per N in global memory, read through
 // the read-only cache -- lines spread over several lanes (96..256; lane-dependent
 // indices would serialise on the constant cache) and the primes 83 and 97 of the
@@ -120,6 +125,8 @@ extern __constant__ double2 c_tw_d[fft3d::TW_ENTRIES];
 extern __constant__ float2 c_tw_f[fft3d::TW_ENTRIES];
 extern __constant__ double2 c_rader17_d[fft3d::RADER17_ENTRIES];
 extern __constant__ float2 c_rader17_f[fft3d::RADER17_ENTRIES];
+extern __constant__ double c_crt17_d[fft3d::CRT17_ENTRIES];
+extern __constant__ float c_crt17_f[fft3d::CRT17_ENTRIES];
 #endif
 #if defined(__CUDACC__)
 extern __device__ double2 g_twbig_d[fft3d::TWBIG_ENTRIES];
@@ -131,6 +138,8 @@ extern double2 h_twbig_d[fft3d::TWBIG_ENTRIES];
 extern float2 h_twbig_f[fft3d::TWBIG_ENTRIES];
 extern double2 h_rader17_d[fft3d::RADER17_ENTRIES];
 extern float2 h_rader17_f[fft3d::RADER17_ENTRIES];
+extern double h_crt17_d[fft3d::CRT17_ENTRIES];
+extern float h_crt17_f[fft3d::CRT17_ENTRIES];
 
 namespace fft3d {
 
@@ -153,6 +162,14 @@ struct Tab<double> {
         return c_rader17_d[i];
 #else
         return h_rader17_d[i];
+#endif
+    }
+    FFT_HD static double crt17(int i)
+    {
+#if defined(__CUDA_ARCH__)
+        return c_crt17_d[i];
+#else
+        return h_crt17_d[i];
 #endif
     }
     FFT_HD static double2 twbig(int i)
@@ -181,6 +198,14 @@ struct Tab<float> {
         return c_rader17_f[i];
 #else
         return h_rader17_f[i];
+#endif
+    }
+    FFT_HD static float crt17(int i)
+    {
+#if defined(__CUDA_ARCH__)
+        return c_crt17_f[i];
+#else
+        return h_crt17_f[i];
 #endif
     }
     FFT_HD static float2 twbig(int i)
@@ -240,6 +265,7 @@ FFT_HD cx<T> ctwiddle(cx<T> a, int E)
 
 constexpr int ALG_DEFAULT = 0;
 constexpr int ALG_RADER = 1;
+constexpr int ALG_CRT = 2;
 
 template <int N, int S, typename T, int ALG = ALG_DEFAULT>
 FFT_HD void dft(cx<T> *v);
@@ -388,6 +414,95 @@ FFT_HD void dft17_rader(cx<T> *v)
     for (int s = 0; s < 16; ++s) v[rader17_pow((16 - s) % 16)] = a[s];
 }
 
+// 17-point DFT, ALG_CRT: the conjugate-pair folded form of dft_odd_folded with
+// its cosine half computed as a cyclic convolution.  The non-zero residues mod 17
+// are +-3^a, a = 0..7 (3 is a primitive root, 3^8 = -1): with j_a = +-3^a in
+// 1..8 (sign e_a), u_a = v[j_a] + v[17 - j_a] and w_a = e_a (v[j_a] - v[17 - j_a]),
+//   cosine sums  A_b = x0 + sum_a u_a c[(a + b) mod 8],   c[m] = cos(2 pi 3^m / 17)
+//   sine sums    B_b = e_b sum_a w_a s~[a + b],   s~[m] = s[m], s~[m + 8] = -s[m],
+//                s[m] = sin(2 pi 3^m / 17)
+// (Rader's re-indexing, folded to the 8 classes +-3^a).  The cosine correlation
+// runs as the convolution of u reversed with c through the split
+// x^8 - 1 = (x - 1)(x + 1)(x^2 + 1)(x^4 + 1): 14 additions reduce the input, 22
+// products against the kernel's residues (a plan-time table with the
+// reconstruction's halvings folded in; x0 rides on the x - 1 product) and 14
+// additions rebuild the 8 sums -- 50 operations a real component instead of the
+// 64 multiply-adds of the direct sum.  The sine half stays direct.
+template <int S, typename T>
+FFT_HD void dft17_crt(cx<T> *v)
+{
+    constexpr int J[8] = {1, 3, 8, 7, 4, 5, 2, 6};         // +-3^a mod 17 in 1..8
+    constexpr int E[8] = {1, 1, -1, -1, -1, 1, -1, -1};    // its sign
+    constexpr int P3[8] = {1, 3, 9, 10, 13, 5, 15, 11};    // 3^a mod 17
+    cx<T> U[8], W[8];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+        U[a] = cadd(v[J[a]], v[17 - J[a]]);
+        W[a] = E[a] > 0 ? csub(v[J[a]], v[17 - J[a]]) : csub(v[17 - J[a]], v[J[a]]);
+    }
+    const cx<T> x0 = v[0];
+    cx<T> sum = x0;
+#pragma unroll
+    for (int a = 0; a < 8; ++a) sum = cadd(sum, U[a]);
+    // cosine half: y = V (*) c mod x^8 - 1 with V_i = U[(8 - i) mod 8]
+    cx<T> P[4], Q[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const cx<T> lo = U[(8 - i) % 8], hi = U[(8 - i - 4) % 8];
+        P[i] = cadd(lo, hi);
+        Q[i] = csub(lo, hi);
+    }
+    const cx<T> P10 = cadd(P[0], P[2]), P11 = cadd(P[1], P[3]);
+    const cx<T> P20 = csub(P[0], P[2]), P21 = csub(P[1], P[3]);
+    const cx<T> e0 = cadd(P10, P11), e1 = csub(P10, P11);
+    const T k0 = Tab<T>::crt17(0), k1 = Tab<T>::crt17(1), k20 = Tab<T>::crt17(2), k21 = Tab<T>::crt17(3);
+    const cx<T> f0 = {x0.re + e0.re * k0, x0.im + e0.im * k0};
+    const cx<T> f1 = cscale(e1, k1);
+    const cx<T> F20 = {P20.re * k20 - P21.re * k21, P20.im * k20 - P21.im * k21};
+    const cx<T> F21 = {P20.re * k21 + P21.re * k20, P20.im * k21 + P21.im * k20};
+    cx<T> FQ[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        cx<T> acc = {T(0), T(0)};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const T kq = m - i >= 0 ? Tab<T>::crt17(4 + m - i) : -Tab<T>::crt17(8 + m - i);
+            acc.re += Q[i].re * kq;
+            acc.im += Q[i].im * kq;
+        }
+        FQ[m] = acc;
+    }
+    const cx<T> Y10 = cadd(f0, f1), Y11 = csub(f0, f1);
+    const cx<T> YP[4] = {cadd(Y10, F20), cadd(Y11, F21), csub(Y10, F20), csub(Y11, F21)};
+    cx<T> A[8];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+        A[b] = cadd(YP[b], FQ[b]);
+        A[b + 4] = csub(YP[b], FQ[b]);
+    }
+    // sine half, direct
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+        cx<T> B = {T(0), T(0)};
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+            const int m = a + b;
+            const T sm = m < 8 ? line_tw<17, T>(P3[m]).y : -line_tw<17, T>(P3[m - 8]).y;
+            B.re += W[a].re * sm;
+            B.im += W[a].im * sm;
+        }
+        const cx<T> ib = cmul_iS<S>(B);
+        if (E[b] > 0) {
+            v[J[b]] = cadd(A[b], ib);
+            v[17 - J[b]] = csub(A[b], ib);
+        } else {
+            v[J[b]] = csub(A[b], ib);
+            v[17 - J[b]] = cadd(A[b], ib);
+        }
+    }
+    v[0] = sum;
+}
+
 template <int N, int S, typename T, int ALG>
 FFT_HD void dft(cx<T> *v)
 {
@@ -407,6 +522,8 @@ FFT_HD void dft(cx<T> *v)
         v[3] = csub(d02, d13);
     } else if constexpr (N == 17 && ALG == ALG_RADER) {
         dft17_rader<S, T>(v);
+    } else if constexpr (N == 17 && ALG == ALG_CRT) {
+        dft17_crt<S, T>(v);
     } else if constexpr (ce_is_prime(N)) {
         dft_odd_folded<N, S, T>(v);
     } else {

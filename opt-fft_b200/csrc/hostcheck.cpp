@@ -498,6 +498,8 @@ static const EmuEntry kEmu[] = {
     EMU(9, 25, 7, float, 0, 3),    EMU(20, 12, 6, float, 0, 3),  EMU(11, 4, 9, float, 0, 15),
     EMU_TP(30, 30, 30, double, 3), EMU_TP(30, 30, 30, double, 5),
     EMU_BST(17, 17, 17, double, 0, 1), EMU_BST(17, 17, 17, float, 0, 2),
+    EMU(17, 17, 17, double, 2, 1),     EMU(17, 17, 17, float, 2, 2),
+    EMU_BST(17, 17, 17, double, 2, 1), EMU_BST(17, 17, 17, float, 2, 2),
     EMU_BST(13, 13, 13, double, 0, 1), EMU_BST(13, 13, 13, double, 0, 2),
     EMU_BST(13, 13, 13, float, 0, 2),  EMU_BST(8, 8, 8, double, 0, 1),
     EMU_BST(16, 16, 16, double, 0, 1), EMU_BST(16, 16, 16, float, 0, 1),

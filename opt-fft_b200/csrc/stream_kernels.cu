@@ -275,6 +275,7 @@ void register_stream_kernels(std::vector<KernelEntry> &out)
     FFT3D_STREAM(17, 17, 17, double, 1, 1, 320, 2, 1);
     FFT3D_STREAM(17, 17, 17, double, 0, 1, 320, 1, 2);
     FFT3D_STREAM_BST(17, 17, 17, double, 0, 1, 320, 2, 1);
+    FFT3D_STREAM_BST(17, 17, 17, double, 2, 1, 320, 2, 1);  // CRT cosine half
     FFT3D_STREAM(8, 8, 16, double, 0, 4, 512, 2, 1);
     FFT3D_STREAM(8, 8, 16, double, 0, 2, 256, 4, 1);
     FFT3D_STREAM(13, 13, 13, double, 0, 1, 192, 3, 2);
@@ -294,6 +295,7 @@ void register_stream_kernels(std::vector<KernelEntry> &out)
     FFT3D_STREAM(17, 17, 17, float, 0, 2, 640, 2, 1);
     FFT3D_STREAM(17, 17, 17, float, 1, 2, 640, 2, 1);
     FFT3D_STREAM_BST(17, 17, 17, float, 0, 2, 640, 2, 1);
+    FFT3D_STREAM_BST(17, 17, 17, float, 2, 2, 640, 2, 1);
     FFT3D_STREAM(8, 8, 16, float, 0, 4, 512, 4, 1);
     FFT3D_STREAM(8, 8, 16, float, 0, 8, 512, 2, 1);
     FFT3D_STREAM(16, 16, 32, float, 0, 1, 256, 2, 1);

@@ -8,6 +8,8 @@ __constant__ double2 c_tw_d[fft3d::TW_ENTRIES];
 __constant__ float2 c_tw_f[fft3d::TW_ENTRIES];
 __constant__ double2 c_rader17_d[fft3d::RADER17_ENTRIES];
 __constant__ float2 c_rader17_f[fft3d::RADER17_ENTRIES];
+__constant__ double c_crt17_d[fft3d::CRT17_ENTRIES];
+__constant__ float c_crt17_f[fft3d::CRT17_ENTRIES];
 __device__ double2 g_twbig_d[fft3d::TWBIG_ENTRIES];
 __device__ float2 g_twbig_f[fft3d::TWBIG_ENTRIES];
 
@@ -27,6 +29,9 @@ int ensure_device_tables(int device)
     if (cudaMemcpyToSymbol(c_rader17_d, h_rader17_d, sizeof(h_rader17_d)) != cudaSuccess)
         return FFT3D_B200_ERR_CUDA;
     if (cudaMemcpyToSymbol(c_rader17_f, h_rader17_f, sizeof(h_rader17_f)) != cudaSuccess)
+        return FFT3D_B200_ERR_CUDA;
+    if (cudaMemcpyToSymbol(c_crt17_d, h_crt17_d, sizeof(h_crt17_d)) != cudaSuccess ||
+        cudaMemcpyToSymbol(c_crt17_f, h_crt17_f, sizeof(h_crt17_f)) != cudaSuccess)
         return FFT3D_B200_ERR_CUDA;
     if (cudaMemcpyToSymbol(g_twbig_d, h_twbig_d, sizeof(h_twbig_d)) != cudaSuccess ||
         cudaMemcpyToSymbol(g_twbig_f, h_twbig_f, sizeof(h_twbig_f)) != cudaSuccess)

@@ -3,7 +3,9 @@
 // fft3d_create() does all table work (bench/geom/fft3d_api.h:30-32): the
 // cos/sin(2*pi*e/N) table for every extent N <= 64 with the exponent reduced mod N
 // (python/fft3d.py:139-148), and the Rader-17 kernel spectrum
-// K = FFT16(brev)/16 with brev[t] = W17^{3^-t} (python/fft3d.py:229-238), are
+// K = FFT16(brev)/16 with brev[t] = W17^{3^-t} (python/fft3d.py:229-238), and the
+// residues of the cosine kernel c[m] = cos(2*pi*3^m/17) that dft17_crt multiplies
+// by (mod x-1 and x+1 scaled 1/8, mod x^2+1 scaled 1/4, mod x^4+1 scaled 1/2), are
 // evaluated in x87 extended precision, rounded once to double and to float, and
 // copied by tables.cu to __constant__ memory of each device the first time a plan
 // is created on it.
@@ -16,6 +18,8 @@ double2 h_tw_d[fft3d::TW_ENTRIES];
 float2 h_tw_f[fft3d::TW_ENTRIES];
 double2 h_rader17_d[fft3d::RADER17_ENTRIES];
 float2 h_rader17_f[fft3d::RADER17_ENTRIES];
+double h_crt17_d[fft3d::CRT17_ENTRIES];
+float h_crt17_f[fft3d::CRT17_ENTRIES];
 double2 h_twbig_d[fft3d::TWBIG_ENTRIES];
 float2 h_twbig_f[fft3d::TWBIG_ENTRIES];
 
@@ -83,6 +87,25 @@ static void fill_host_tables()
             h_rader17_d[si * 16 + k] = make_double2((double)re, (double)im);
             h_rader17_f[si * 16 + k] = make_float2((float)re, (float)im);
         }
+    }
+    // CRT-17 cosine-kernel residues
+    long double c[8];
+    for (int m = 0; m < 8; ++m) {
+        long double s;
+        exact_cis(pw[m], 17, &c[m], &s);
+    }
+    long double P[4], Q[4];
+    for (int i = 0; i < 4; ++i) {
+        P[i] = c[i] + c[i + 4];  // mod x^4 - 1
+        Q[i] = c[i] - c[i + 4];  // mod x^4 + 1
+    }
+    const long double P10 = P[0] + P[2], P11 = P[1] + P[3];  // mod x^2 - 1
+    const long double res[8] = {(P10 + P11) / 8.0L, (P10 - P11) / 8.0L,      // mod x - 1, x + 1
+                                (P[0] - P[2]) / 4.0L, (P[1] - P[3]) / 4.0L,  // mod x^2 + 1
+                                Q[0] / 2.0L, Q[1] / 2.0L, Q[2] / 2.0L, Q[3] / 2.0L};
+    for (int i = 0; i < 8; ++i) {
+        h_crt17_d[i] = (double)res[i];
+        h_crt17_f[i] = (float)res[i];
     }
 }
 

@@ -25,7 +25,7 @@ GEOMS = [((6, 6, 6), 0, 16), ((8, 8, 8), 0, 8), ((12, 12, 12), 0, 2), ((16, 16, 
          ((9, 9, 9), 0, 2), ((5, 8, 12), 0, 1), ((32, 8, 4), 0, 1), ((13, 5, 8), 0, 1),
          ((4, 4, 4), 0, 2), ((1, 8, 8), 0, 1), ((8, 1, 8), 0, 1), ((8, 8, 1), 0, 1),
          ((1, 1, 1), 0, 1), ((3, 3, 3), 0, 1), ((17, 2, 2), 0, 1), ((13, 13, 13), 0, 2),
-         ((23, 23, 23), 0, 1),
+         ((23, 23, 23), 0, 1), ((17, 17, 17), 2, 1),
          # the group sizes of the VOLUME kernels for the reference's other extents
          ((1, 1, 1), 0, 64), ((3, 3, 3), 0, 32), ((4, 4, 4), 0, 16), ((9, 9, 9), 0, 4),
          ((10, 10, 10), 0, 2), ((15, 15, 15), 0, 1), ((2, 3, 5), 0, 32), ((5, 8, 12), 0, 4),
@@ -39,7 +39,8 @@ GEOMS = [((6, 6, 6), 0, 16), ((8, 8, 8), 0, 8), ((12, 12, 12), 0, 2), ((16, 16, 
          ((16, 3, 5), 0, 12), ((24, 18, 12), 0, 1), ((2, 2, 64), 0, 12), ((64, 2, 2), 0, 8),
          ((9, 25, 7), 0, 1), ((20, 12, 6), 0, 1), ((11, 4, 9), 0, 7)]
 GEOMS64 = [((6, 6, 6), 0, 32), ((8, 8, 8), 0, 16), ((12, 12, 12), 0, 4), ((16, 16, 16), 0, 2),
-           ((17, 17, 17), 0, 2), ((17, 17, 17), 1, 2), ((24, 24, 24), 0, 1), ((8, 8, 16), 0, 16),
+           ((17, 17, 17), 0, 2), ((17, 17, 17), 1, 2), ((17, 17, 17), 2, 2),
+           ((24, 24, 24), 0, 1), ((8, 8, 16), 0, 16),
            ((16, 16, 32), 0, 1), ((36, 36, 36), 0, 1), ((13, 13, 13), 0, 4), ((23, 23, 23), 0, 1),
            ((1, 1, 1), 0, 128), ((3, 3, 3), 0, 64), ((4, 4, 4), 0, 32), ((9, 9, 9), 0, 8),
            ((10, 10, 10), 0, 4), ((15, 15, 15), 0, 2), ((2, 3, 5), 0, 64), ((7, 11, 13), 0, 4),
@@ -125,6 +126,20 @@ def test_stream_bulk_store_item(hostcheck, shape, prec, vpc, nvol, sign):
     want = oracle.fft3d(x64) if sign < 0 else oracle.ifft3d(x64)
     err = oracle.rel_error_per_volume(got, want).max()
     assert err < (C128_TOL if prec == 0 else C64_TOL), err
+
+
+@pytest.mark.parametrize("prec,vpc", [(0, 1), (1, 2)])
+@pytest.mark.parametrize("sign", [-1, +1])
+def test_stream_bulk_store_crt17(hostcheck, prec, vpc, sign):
+    """The bulk-store item with the CRT 17-point codelet (alg = 400 + 2)."""
+    shape = (17, 17, 17)
+    rng = np.random.default_rng(3700 + prec)
+    dt = np.complex128 if prec == 0 else np.complex64
+    x = field(rng, (3,) + shape, dtype=dt)
+    got = run(hostcheck, x, shape, prec, sign, 402, vpc)
+    x64 = x.astype(np.complex128)
+    want = oracle.fft3d(x64) if sign < 0 else oracle.ifft3d(x64)
+    assert oracle.rel_error_per_volume(got, want).max() < (C128_TOL if prec == 0 else C64_TOL)
 
 
 @pytest.mark.parametrize("n,prec,pl", [(36, 0, 4), (36, 1, 6), (36, 1, 4)])

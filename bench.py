@@ -548,7 +548,13 @@ def measure_serve(fb, torch, device, n_req=1_000_000, seed=2024, arena_gb=(24, 4
     psat = run(fb.SERVE_PLAIN, None, True, 32)
     out["plain_fp64_saturation"] = psat
     out["plain_fp64_poisson_same_rate"] = run(fb.SERVE_PLAIN, lam, True, 32)
-    out["plain_fp64_poisson_own_rate"] = run(fb.SERVE_PLAIN, 0.7 * psat["requests_per_s"], True, 32)
+    # the baseline's latency at its own sustainable rate, measured like the
+    # headline: three runs, the run with the median p99 reported
+    pruns = sorted((run(fb.SERVE_PLAIN, 0.7 * psat["requests_per_s"], True, 32) for _ in range(3)),
+                   key=lambda r: r["p99_s"])
+    pruns[1]["p99_runs_s"] = [r["p99_s"] for r in pruns]
+    pruns[1]["p50_runs_s"] = [r["p50_s"] for r in pruns]
+    out["plain_fp64_poisson_own_rate"] = pruns[1]
     out["throughput_ratio_saturation"] = sat["volumes_per_s"] / psat["volumes_per_s"]
     del buf
     return out

@@ -62,16 +62,19 @@ __device__ __forceinline__ void batch_load(cx<typename G::T> *sm, const cx<typen
     cp_async_commit();
 }
 
+// Line route per extent: 17-point lines take the CRT form of the folded sum.
+constexpr int batch_alg(int n) { return n == 17 ? ALG_CRT : ALG_DEFAULT; }
+
 template <int NT, class G, int S>
 __device__ __forceinline__ void batch_passes(cx<typename G::T> *sm, int nv,
                                              cx<typename G::T> *gout, typename G::T scale)
 {
     const int tid = threadIdx.x;
-    for (int r = tid; r < nv * G::ROWS; r += NT) pass_z<G, S, ALG_DEFAULT>(sm, r);
+    for (int r = tid; r < nv * G::ROWS; r += NT) pass_z<G, S, batch_alg(G::N2)>(sm, r);
     __syncthreads();
-    for (int l = tid; l < nv * G::N0 * G::N2; l += NT) pass_y<G, S, ALG_DEFAULT>(sm, l);
+    for (int l = tid; l < nv * G::N0 * G::N2; l += NT) pass_y<G, S, batch_alg(G::N1)>(sm, l);
     __syncthreads();
-    for (int l = tid; l < nv * G::N1 * G::N2; l += NT) pass_x_out<G, S, ALG_DEFAULT>(sm, l, gout, scale);
+    for (int l = tid; l < nv * G::N1 * G::N2; l += NT) pass_x_out<G, S, batch_alg(G::N0)>(sm, l, gout, scale);
 }
 
 // ---------------------------------------------------------------- two-phase large cube
